@@ -1,0 +1,179 @@
+// xmpIntegersMul[Async] (replaces src/mul.cu:26-303 and the kernels
+// regmp_mul/sqr_kernel, digitmp_mul/sqr_kernel, implementations.h:250-434,
+// with RegMP mul (regmp/mul_imad.h:26-103) and DigitMP mul (digitmp/mul.h)).
+//
+// p = a * b mod 2^P(p), operands zero-extended; P(p) >= max(P(a), P(b)).
+// Register path: the larger operand is held in registers as AL limbs, the
+// smaller as BL limbs (AL, BL from a small set of classes), and the AL+BL-limb
+// product is formed by operand scanning, one row of two mad chains (low and
+// high halves) per limb of the smaller operand.  Large path (either operand
+// above 32 limbs): product scanning straight from the interleaved arrays with
+// a three-word column accumulator, so nothing has to fit in registers.
+// Squaring (a == b without index arrays, src/mul.cu:147-149) takes the same
+// kernels.
+#include "internal.h"
+#include "carry.cuh"
+#include <algorithm>
+
+using namespace xmpb;
+
+namespace xmpb {
+
+template <int N>
+__device__ __forceinline__ uint32_t at(const uint32_t (&x)[N], int i) {
+  return i < N ? x[i < N ? i : 0] : 0u;
+}
+
+template <int L>
+__device__ __forceinline__ void load_limbs(uint32_t (&x)[L], const ArrayView &v, uint32_t e) {
+#pragma unroll
+  for (int g = 0; g < (L + 3) / 4; g++) {
+    uint4 q = load_group(v.limbs, v.nlimbs, v.stride, e, g);
+    if (4 * g + 0 < L) x[(4 * g + 0) < L ? 4 * g + 0 : 0] = q.x;
+    if (4 * g + 1 < L) x[(4 * g + 1) < L ? 4 * g + 1 : 0] = q.y;
+    if (4 * g + 2 < L) x[(4 * g + 2) < L ? 4 * g + 2 : 0] = q.z;
+    if (4 * g + 3 < L) x[(4 * g + 3) < L ? 4 * g + 3 : 0] = q.w;
+  }
+}
+
+template <int N>
+__device__ __forceinline__ void store_limbs(const uint32_t (&x)[N], const OutView &c, uint32_t e) {
+  uint32_t groups = div_up(c.nlimbs, 4);
+#pragma unroll
+  for (int g = 0; g < (N + 3) / 4; g++)
+    if ((uint32_t)g < groups)
+      store_group(c.limbs, c.nlimbs, c.stride, e, g, make_uint4(at(x, 4 * g), at(x, 4 * g + 1), at(x, 4 * g + 2), at(x, 4 * g + 3)));
+  for (uint32_t g = (N + 3) / 4; g < groups; g++) store_group(c.limbs, c.nlimbs, c.stride, e, g, make_uint4(0, 0, 0, 0));
+}
+
+template <int AL, int BL>
+__global__ void __launch_bounds__(128) mul_reg_kernel(ArrayView a, ArrayView b, OutView c, uint32_t count) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  uint32_t ea = in_element(a, i), eb = in_element(b, i), ec = out_element(c, i);
+  if (ec >= c.count) return;
+  uint32_t A[AL], B[BL], P[AL + BL];
+  load_limbs<AL>(A, a, ea);
+  load_limbs<BL>(B, b, eb);
+#pragma unroll
+  for (int k = 0; k < AL + BL; k++) P[k] = 0;
+#pragma unroll
+  for (int j = 0; j < BL; j++) {
+    uint32_t w = B[j];
+    P[j] = mad_lo_cc(A[0], w, P[j]);
+#pragma unroll
+    for (int k = 1; k < AL; k++) P[j + k] = madc_lo_cc(A[k], w, P[j + k]);
+    P[j + AL] = addc(0u, 0u);
+    P[j + 1] = mad_hi_cc(A[0], w, P[j + 1]);
+#pragma unroll
+    for (int k = 1; k < AL - 1; k++) P[j + 1 + k] = madc_hi_cc(A[k], w, P[j + 1 + k]);
+    P[j + AL] = madc_hi(A[AL - 1], w, P[j + AL]);
+  }
+  store_limbs<AL + BL>(P, c, ec);
+}
+
+// Column k of the product, accumulated from the interleaved arrays.
+__global__ void __launch_bounds__(128) mul_stream_kernel(ArrayView a, ArrayView b, OutView c, uint32_t count) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  uint32_t ea = in_element(a, i), eb = in_element(b, i), ec = out_element(c, i);
+  if (ec >= c.count) return;
+  const int32_t na = a.nlimbs, nb = b.nlimbs;
+  uint32_t c0 = 0, c1 = 0, c2 = 0;
+  uint32_t groups = div_up(c.nlimbs, 4);
+  for (uint32_t g = 0; g < groups; g++) {
+    uint32_t out[4];
+    for (int q = 0; q < 4; q++) {
+      int32_t k = g * 4 + q;
+      int32_t lo = max(0, k - nb + 1), hi = min(k, na - 1);
+      for (int32_t t = lo; t <= hi; t++) {
+        uint32_t x = load_limb(a.limbs, a.nlimbs, a.stride, ea, t);
+        uint32_t y = load_limb(b.limbs, b.nlimbs, b.stride, eb, k - t);
+        c0 = mad_lo_cc(x, y, c0);
+        c1 = madc_hi_cc(x, y, c1);
+        c2 = addc(c2, 0u);
+      }
+      out[q] = c0;
+      c0 = c1;
+      c1 = c2;
+      c2 = 0;
+    }
+    store_group(c.limbs, c.nlimbs, c.stride, ec, g, make_uint4(out[0], out[1], out[2], out[3]));
+  }
+}
+
+typedef void (*MulLaunch)(ArrayView, ArrayView, OutView, uint32_t, cudaStream_t);
+template <int AL, int BL>
+static void launch_mul(ArrayView a, ArrayView b, OutView c, uint32_t count, cudaStream_t s) {
+  mul_reg_kernel<AL, BL><<<grid_for(count, 128), 128, 0, s>>>(a, b, c, count);
+}
+
+static const int kClasses[] = {2, 4, 8, 12, 16, 24, 32};
+static int class_of(uint32_t n) {
+  for (int c : kClasses)
+    if (n <= (uint32_t)c) return c;
+  return 0;
+}
+
+#define XMPB_MUL_CASE(A, B) \
+  if (al == A && bl == B) return launch_mul<A, B>;
+static MulLaunch pick_mul(int al, int bl) {
+  XMPB_MUL_CASE(2, 2) XMPB_MUL_CASE(4, 2) XMPB_MUL_CASE(4, 4) XMPB_MUL_CASE(8, 2) XMPB_MUL_CASE(8, 4)
+  XMPB_MUL_CASE(8, 8) XMPB_MUL_CASE(12, 2) XMPB_MUL_CASE(12, 4) XMPB_MUL_CASE(12, 8) XMPB_MUL_CASE(12, 12)
+  XMPB_MUL_CASE(16, 2) XMPB_MUL_CASE(16, 4) XMPB_MUL_CASE(16, 8) XMPB_MUL_CASE(16, 12) XMPB_MUL_CASE(16, 16)
+  XMPB_MUL_CASE(24, 2) XMPB_MUL_CASE(24, 4) XMPB_MUL_CASE(24, 8) XMPB_MUL_CASE(24, 12) XMPB_MUL_CASE(24, 16)
+  XMPB_MUL_CASE(24, 24) XMPB_MUL_CASE(32, 2) XMPB_MUL_CASE(32, 4) XMPB_MUL_CASE(32, 8) XMPB_MUL_CASE(32, 12)
+  XMPB_MUL_CASE(32, 16) XMPB_MUL_CASE(32, 24) XMPB_MUL_CASE(32, 32)
+  return nullptr;
+}
+
+}  // namespace xmpb
+
+extern "C" {
+
+xmpError_t XMPAPI xmpIntegersMulAsync(xmpHandle_t h, xmpIntegers_t p, const xmpIntegers_t a, const xmpIntegers_t b,
+                                       uint32_t count) {
+  if (!h || !p || !a || !b) return xmpErrorInvalidParameter;
+  int dev = h->device;
+  if (p->device != dev || a->device != dev || b->device != dev) return xmpErrorInvalidDevice;
+  if (count == 0) return xmpErrorSuccess;
+  DeviceGuard guard(dev);
+  xmpExecutionPolicy_t pol = h->policy;
+  if (p->count < count) return xmpErrorInvalidCount;
+  if (pol->indices[0] && pol->indices_count[0] < count) return xmpErrorInvalidCount;
+  if (p->precision < std::max(a->precision, b->precision)) return xmpErrorInvalidPrecision;
+
+  ArrayView va = view_in(a, pol->indices[1], pol->indices_count[1]);
+  ArrayView vb = view_in(b, pol->indices[2], pol->indices_count[2]);
+  // Larger operand first (register rows run over the smaller one).
+  if (va.nlimbs < vb.nlimbs) std::swap(va, vb);
+  int al = class_of(va.nlimbs), bl = class_of(vb.nlimbs);
+  MulLaunch launch = nullptr;
+  if (al && bl && pol->algorithm != xmpAlgorithmDigitMP) launch = pick_mul(al, bl);
+  if (pol->algorithm == xmpAlgorithmRegMP && !launch) return xmpErrorUnsupported;
+  bool aliased = (p == a || p == b);
+  bool indexed = pol->indices[0] || pol->indices[1] || pol->indices[2];
+  OutTarget t;
+  // The streamed kernel reads inputs while writing the product: stage whenever it aliases.
+  xmpError_t e = begin_output(h, p, aliased, indexed || !launch, &t);
+  if (e != xmpErrorSuccess) return e;
+  OutView vc = view_out(p, t.limbs, pol->indices[0]);
+  if (launch)
+    launch(va, vb, vc, count, h->stream);
+  else
+    mul_stream_kernel<<<grid_for(count, 128), 128, 0, h->stream>>>(va, vb, vc, count);
+  e = end_output(h, p, t);
+  if (e != xmpErrorSuccess) return e;
+  return check_cuda();
+}
+
+xmpError_t XMPAPI xmpIntegersMul(xmpHandle_t h, xmpIntegers_t p, const xmpIntegers_t a, const xmpIntegers_t b,
+                                  uint32_t count) {
+  xmpError_t e = xmpIntegersMulAsync(h, p, a, b, count);
+  if (e != xmpErrorSuccess) return e;
+  DeviceGuard guard(h->device);
+  cudaStreamSynchronize(h->stream);
+  return check_cuda();
+}
+
+}  // extern "C"

@@ -1,0 +1,179 @@
+// Host dispatch of xmpIntegersPowm[Async] (replaces src/powm.cu:61-307 and
+// src/include/powm_operators.h:15-455).  Validation and index semantics are the
+// reference's: out/base/mod precisions equal, exponent precision free, output
+// index = indices[0][i], base/exp/mod = indices[1..3][i % n] % array count.
+// The configuration (distribution, lanes per instance, limbs per lane, window)
+// comes from the handle's tuner when it has an entry for the size class,
+// otherwise from a register/occupancy heuristic; the reference's static
+// Maxwell/Kepler latency tables (powm.cu:120-236) have no counterpart.
+#include "powm.h"
+#include <algorithm>
+#include <math.h>
+
+using namespace xmpb;
+
+namespace xmpb {
+
+std::vector<PowmKernelEntry> &powm_registry() {
+  static std::vector<PowmKernelEntry> r;
+  return r;
+}
+
+const PowmKernelEntry *powm_find(int tpi, int limbs) {
+  for (const auto &e : powm_registry())
+    if (e.tpi == tpi && e.limbs == limbs) return &e;
+  return nullptr;
+}
+
+int window_for_bits(uint32_t exp_bits) {
+  if (exp_bits <= 1) return 1;
+  int best = 1;
+  double best_cost = 1e300;
+  for (int w = 1; w <= 7; w++) {
+    double cost = (double)((1 << w) - 2) + ceil((double)exp_bits / w);
+    if (cost < best_cost - 1e-9) {
+      best_cost = cost;
+      best = w;
+    }
+  }
+  return best;
+}
+
+bool powm_config_valid(const PowmConfig &c, uint32_t nlimbs) {
+  if (c.window < 1 || c.window > 7) return false;
+  if (c.dist == kDistDigit) return true;
+  if ((uint64_t)c.tpi * c.limbs < nlimbs) return false;
+  return powm_find(c.tpi, c.limbs) != nullptr;
+}
+
+PowmConfig powm_default_config(uint32_t nlimbs, uint32_t exp_bits, uint32_t count, xmpAlgorithm_t alg,
+                               uint32_t sm_count) {
+  PowmConfig best;
+  best.window = window_for_bits(exp_bits);
+  if (alg == xmpAlgorithmDigitMP) {
+    best.dist = kDistDigit;
+    return best;
+  }
+  // Enough lanes to give every SM a few warps; below that, spread instances wider.
+  const double want_threads = (double)sm_count * 4 * 32;
+  double best_score = 1e300;
+  for (const auto &e : powm_registry()) {
+    if (alg == xmpAlgorithmRegMP && e.tpi != 1) continue;
+    if (alg == xmpAlgorithmDistributedMP && e.tpi == 1) continue;
+    uint32_t cap = (uint32_t)e.tpi * e.limbs;
+    if (cap < nlimbs) continue;
+    // Work per instance grows with capacity^2; lane overhead (shfl, carry
+    // bookkeeping) is ~12 instructions per 4L multiply-adds.
+    double pad = (double)cap / nlimbs;
+    double work = pad * pad * (4.0 * e.limbs + (e.tpi > 1 ? 12.0 : 4.0)) / (4.0 * e.limbs);
+    double threads = (double)count * e.tpi;
+    double starve = threads < want_threads ? want_threads / threads : 1.0;
+    double regs = e.limbs > 16 && e.tpi > 1 ? 1.5 : 1.0;  // register pressure beyond 16 limbs
+    double score = work * starve * regs;
+    if (score < best_score) {
+      best_score = score;
+      best.tpi = e.tpi;
+      best.limbs = e.limbs;
+    }
+  }
+  // Larger than every register kernel: the digit-serial kernel takes any size,
+  // unless the caller forced a register distribution (then Unsupported).
+  if (best.tpi == 0 && alg == xmpAlgorithmDefault) best.dist = kDistDigit;
+  return best;
+}
+
+size_t powm_table_bytes(const PowmConfig &cfg, uint32_t nlimbs, uint32_t count) {
+  if (cfg.dist == kDistDigit) {
+    // table + N, x, b, m, r, r2 working arrays, all nlimbs+2 words per instance
+    size_t words = ((size_t)1 << cfg.window) * nlimbs + 6 * ((size_t)nlimbs + 2);
+    return words * 4 * round_up(count, 128);
+  }
+  size_t threads = round_up((uint32_t)std::min<uint64_t>((uint64_t)count * cfg.tpi, 0xffffff80ull), 128);
+  return threads * (size_t)cfg.limbs * ((size_t)1 << cfg.window) * 4;
+}
+
+xmpError_t powm_run(xmpHandle_t h, const PowmConfig &cfg0, const OutView &out, const ArrayView &base,
+                    const ArrayView &exp, const ArrayView &mod, uint32_t count) {
+  PowmConfig cfg = cfg0;
+  if (cfg.dist == kDistDigit) return powm_digit_run(h, cfg, out, base, exp, mod, count);
+  const PowmKernelEntry *k = powm_find(cfg.tpi, cfg.limbs);
+  if (!k) return xmpErrorUnsupported;
+  size_t limit = scratch_limit(h);
+  // Chunk so the window tables fit; shrink the window if even one block of instances does not fit.
+  uint32_t per_block = 128 / cfg.tpi;
+  uint32_t chunk = count;
+  while (true) {
+    size_t per_inst = (size_t)cfg.tpi * cfg.limbs * ((size_t)1 << cfg.window) * 4;
+    uint64_t fit = limit / per_inst;
+    fit = fit / per_block * per_block;
+    if (fit >= per_block) {
+      chunk = (uint32_t)std::min<uint64_t>(count, fit);
+      break;
+    }
+    if (cfg.window <= 1) return xmpErrorIncreaseScratchLimit;
+    cfg.window--;
+  }
+  xmpError_t e = ensure_scratch(h, powm_table_bytes(cfg, mod.nlimbs, chunk));
+  if (e != xmpErrorSuccess) return e;
+  PowmArgs a;
+  a.base = base;
+  a.exp = exp;
+  a.mod = mod;
+  a.out = out;
+  a.window = cfg.window;
+  a.table = (uint32_t *)h->scratch;
+  for (uint32_t start = 0; start < count; start += chunk) {
+    a.start = start;
+    a.count = std::min(chunk, count - start);
+    int grid = grid_for((uint64_t)a.count * cfg.tpi, 128);
+    k->launch(a, grid, h->stream);
+  }
+  return check_cuda();
+}
+
+}  // namespace xmpb
+
+extern "C" {
+
+xmpError_t XMPAPI xmpIntegersPowmAsync(xmpHandle_t h, xmpIntegers_t out, const xmpIntegers_t base,
+                                        const xmpIntegers_t exp, const xmpIntegers_t mod, uint32_t count) {
+  if (!h || !out || !base || !exp || !mod) return xmpErrorInvalidParameter;
+  int dev = h->device;
+  if (out->device != dev || base->device != dev || exp->device != dev || mod->device != dev)
+    return xmpErrorInvalidDevice;
+  if (count == 0) return xmpErrorSuccess;
+  DeviceGuard guard(dev);
+  xmpExecutionPolicy_t p = h->policy;
+  if (out->count < count) return xmpErrorInvalidCount;
+  if (p->indices[0] && p->indices_count[0] < count) return xmpErrorInvalidCount;
+  if (base->precision != out->precision || mod->precision != out->precision) return xmpErrorInvalidPrecision;
+
+  PowmConfig cfg;
+  bool tuned = (p->algorithm == xmpAlgorithmDefault) && tuner_lookup_powm(h, mod->nlimbs, exp->precision, count, &cfg);
+  if (!tuned) cfg = powm_default_config(mod->nlimbs, exp->precision, count, p->algorithm, h->sm_count);
+  if (!powm_config_valid(cfg, mod->nlimbs)) return xmpErrorUnsupported;
+
+  bool aliased = (out == base || out == exp || out == mod);
+  bool indexed = p->indices[0] || p->indices[1] || p->indices[2] || p->indices[3];
+  OutTarget t;
+  xmpError_t e = begin_output(h, out, aliased, indexed, &t);
+  if (e != xmpErrorSuccess) return e;
+  e = powm_run(h, cfg, view_out(out, t.limbs, p->indices[0]), view_in(base, p->indices[1], p->indices_count[1]),
+               view_in(exp, p->indices[2], p->indices_count[2]), view_in(mod, p->indices[3], p->indices_count[3]),
+               count);
+  if (e != xmpErrorSuccess) return e;
+  e = end_output(h, out, t);
+  if (e != xmpErrorSuccess) return e;
+  return check_cuda();
+}
+
+xmpError_t XMPAPI xmpIntegersPowm(xmpHandle_t h, xmpIntegers_t out, const xmpIntegers_t base, const xmpIntegers_t exp,
+                                   const xmpIntegers_t mod, uint32_t count) {
+  xmpError_t e = xmpIntegersPowmAsync(h, out, base, exp, mod, count);
+  if (e != xmpErrorSuccess) return e;
+  DeviceGuard guard(h->device);
+  cudaStreamSynchronize(h->stream);
+  return check_cuda();
+}
+
+}  // extern "C"

@@ -1,0 +1,69 @@
+// Host-side interface of the powm kernels shared by the dispatcher, the
+// autotuner and the batched (mixed-size) launcher.
+#pragma once
+#include "internal.h"
+#include "powm_kernel.cuh"
+#include <vector>
+
+namespace xmpb {
+
+enum PowmDist : int { kDistLanes = 0, kDistDigit = 1 };
+
+struct PowmConfig {
+  int dist = kDistLanes;  // lanes: TPI x L register kernel; digit: digit-serial kernel
+  int tpi = 0;            // threads per instance (1 = per-thread)
+  int limbs = 0;          // limbs per lane
+  int window = 0;         // window bits
+};
+
+typedef void (*PowmLauncher)(const PowmArgs &args, int grid, cudaStream_t stream);
+
+struct PowmKernelEntry {
+  int tpi;
+  int limbs;
+  PowmLauncher launch;
+  const void *fn;
+};
+
+std::vector<PowmKernelEntry> &powm_registry();
+const PowmKernelEntry *powm_find(int tpi, int limbs);
+
+struct PowmKernelRegistrar {
+  PowmKernelRegistrar(int tpi, int limbs, PowmLauncher l, const void *fn) {
+    powm_registry().push_back(PowmKernelEntry{tpi, limbs, l, fn});
+  }
+};
+
+#define XMPB_REGISTER_POWM(TPI, L)                                                                   \
+  static void powm_launch_##TPI##_##L(const PowmArgs &a, int grid, cudaStream_t s) {                \
+    powm_kernel<TPI, L><<<grid, 128, 0, s>>>(a);                                                     \
+  }                                                                                                   \
+  static PowmKernelRegistrar powm_reg_##TPI##_##L(TPI, L, powm_launch_##TPI##_##L,                  \
+                                                  (const void *)powm_kernel<TPI, L>);
+
+// Best fixed window for a k-bit exponent: minimises table build (2^W - 2
+// multiplies) plus one multiply per window.
+int window_for_bits(uint32_t exp_bits);
+
+// Heuristic configuration for n-limb moduli (used when no tuned entry exists).
+PowmConfig powm_default_config(uint32_t nlimbs, uint32_t exp_bits, uint32_t count, xmpAlgorithm_t alg,
+                               uint32_t sm_count);
+bool powm_config_valid(const PowmConfig &c, uint32_t nlimbs);
+
+// Runs out = base^exp mod mod for `count` op instances starting at 0 with the
+// given configuration (validation already done).  Chunks the launch so the
+// window tables fit the scratch limit.
+xmpError_t powm_run(xmpHandle_t h, const PowmConfig &cfg, const OutView &out, const ArrayView &base,
+                    const ArrayView &exp, const ArrayView &mod, uint32_t count);
+
+// Scratch bytes one launch of `count` instances needs.
+size_t powm_table_bytes(const PowmConfig &cfg, uint32_t nlimbs, uint32_t count);
+
+// Digit-serial kernel launcher (any precision).
+xmpError_t powm_digit_run(xmpHandle_t h, const PowmConfig &cfg, const OutView &out, const ArrayView &base,
+                          const ArrayView &exp, const ArrayView &mod, uint32_t count);
+
+// Configuration chosen by the handle's tuner (selector / exhaustive table), if any.
+bool tuner_lookup_powm(xmpHandle_t h, uint32_t nlimbs, uint32_t exp_bits, uint32_t count, PowmConfig *cfg);
+
+}  // namespace xmpb

@@ -1,0 +1,213 @@
+// Batched modular exponentiation kernel, one template per distribution
+// (TPI lanes per instance x L limbs per lane).
+//
+// Replaces, fused into one launch, the reference's three kernels per chunk
+// (powm_operators.h:105-135): the AR kernel (a*R mod N by division,
+// powm_implementations.h:3-87 / 289-443), the powm kernel running the
+// fixed-window state machine xmp::fwe (powm/powm.h:39-127) and the copy-out
+// kernel (powm_implementations.h:122-152 / 480-516).
+//
+// Per instance:
+//   1. N, n0' = -N^-1 mod 2^32, R^2 mod N (exact doublings + Montgomery squarings)
+//   2. window table T[e] = Mont(x^e), e < 2^W: T[0] = R - N, T[1] = Mont(x),
+//      T[e] = T[e-1]*T[1]; stored in the scratch arena, one contiguous slot
+//      of L limbs per lane so every lane moves its limbs with 128-bit accesses
+//   3. left-to-right fixed window over the exponent: W squarings and one table
+//      multiply per window (window value 0 multiplies by T[0], keeping the
+//      control flow independent of the exponent's bits); the next table entry
+//      is loaded before the squarings so its latency is hidden
+//   4. one Montgomery multiply by 1 and a compare-subtract give x^e mod N
+// The exponent is scanned from the highest window that any instance of the
+// warp needs (warp-uniform, so every shfl sees all 32 lanes); leading zero
+// windows of the reference's full-precision scan (powm_operators.h:55) only
+// square Mont(1) and do not change the result.
+#pragma once
+#include "internal.h"
+#include "mont.cuh"
+
+namespace xmpb {
+
+struct PowmArgs {
+  ArrayView base, exp, mod;
+  OutView out;
+  uint32_t start;   // first op instance of this launch
+  uint32_t count;   // op instances in this launch
+  uint32_t window;  // window bits W, 1..7
+  uint32_t *table;  // scratch: (launch threads / 32) * 32 * L * 2^W words
+};
+
+template <int TPI, int L>
+__device__ __forceinline__ void load_lane_limbs(uint32_t (&x)[L], const uint32_t *limbs, uint32_t nlimbs,
+                                                uint32_t stride, uint32_t e, uint32_t lane) {
+  const uint32_t j0 = lane * L;
+  if (L % 4 == 0) {
+#pragma unroll
+    for (int m = 0; m < L / 4; m++) {
+      uint4 v = load_group(limbs, nlimbs, stride, e, j0 / 4 + m);
+      x[4 * m] = v.x;
+      x[4 * m + 1] = v.y;
+      x[4 * m + 2] = v.z;
+      x[4 * m + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < L; k++) x[k] = load_limb(limbs, nlimbs, stride, e, j0 + k);
+  }
+}
+
+template <int TPI, int L>
+__device__ __forceinline__ void store_lane_limbs(const uint32_t (&x)[L], uint32_t *limbs, uint32_t nlimbs,
+                                                 uint32_t stride, uint32_t e, uint32_t lane) {
+  const uint32_t j0 = lane * L;
+  if (L % 4 == 0) {
+#pragma unroll
+    for (int m = 0; m < L / 4; m++) {
+      uint32_t g = j0 / 4 + m;
+      if (g * 4 < nlimbs) store_group(limbs, nlimbs, stride, e, g, make_uint4(x[4 * m], x[4 * m + 1], x[4 * m + 2], x[4 * m + 3]));
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < L; k++)
+      if (j0 + k < nlimbs) limb_ref(limbs, stride, e, j0 + k) = x[k];
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void slot_store(uint32_t *p, const uint32_t (&x)[L]) {
+  if (L % 4 == 0) {
+#pragma unroll
+    for (int m = 0; m < L / 4; m++)
+      reinterpret_cast<uint4 *>(p)[m] = make_uint4(x[4 * m], x[4 * m + 1], x[4 * m + 2], x[4 * m + 3]);
+  } else if (L % 2 == 0) {
+#pragma unroll
+    for (int m = 0; m < L / 2; m++) reinterpret_cast<uint2 *>(p)[m] = make_uint2(x[2 * m], x[2 * m + 1]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < L; k++) p[k] = x[k];
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void slot_load(const uint32_t *p, uint32_t (&x)[L]) {
+  if (L % 4 == 0) {
+#pragma unroll
+    for (int m = 0; m < L / 4; m++) {
+      uint4 v = reinterpret_cast<const uint4 *>(p)[m];
+      x[4 * m] = v.x;
+      x[4 * m + 1] = v.y;
+      x[4 * m + 2] = v.z;
+      x[4 * m + 3] = v.w;
+    }
+  } else if (L % 2 == 0) {
+#pragma unroll
+    for (int m = 0; m < L / 2; m++) {
+      uint2 v = reinterpret_cast<const uint2 *>(p)[m];
+      x[2 * m] = v.x;
+      x[2 * m + 1] = v.y;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < L; k++) x[k] = p[k];
+  }
+}
+
+// Bits [pos, pos + w) of element e (w <= 8).
+__device__ __forceinline__ uint32_t exp_window(const ArrayView &ex, uint32_t e, uint32_t pos, uint32_t w) {
+  uint32_t j = pos >> 5, sh = pos & 31;
+  uint32_t v = load_limb(ex.limbs, ex.nlimbs, ex.stride, e, j) >> sh;
+  if (sh + w > 32) v |= load_limb(ex.limbs, ex.nlimbs, ex.stride, e, j + 1) << (32 - sh);
+  return v & ((1u << w) - 1u);
+}
+
+// Bit length of the exponent element, scanned by the group's lanes in parallel.
+template <int TPI>
+__device__ __forceinline__ uint32_t exp_bitlen(const Group<TPI> &G, const ArrayView &ex, uint32_t e) {
+  uint32_t bl = 0;
+  for (int32_t j = (int32_t)ex.nlimbs - 1 - (int32_t)G.lane; j >= 0; j -= TPI) {
+    uint32_t v = load_limb(ex.limbs, ex.nlimbs, ex.stride, e, (uint32_t)j);
+    if (v) {
+      bl = (uint32_t)j * 32 + 32 - __clz(v);
+      break;
+    }
+  }
+  return G.seg_max(bl);
+}
+
+template <int TPI, int L>
+__global__ void __launch_bounds__(128) powm_kernel(PowmArgs args) {
+  Group<TPI> G;
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t local = gtid / TPI;
+  const bool valid = local < args.count;
+  // Lanes past the end run a copy of the last instance so every shfl sees a full warp.
+  const uint32_t i = args.start + (valid ? local : args.count - 1);
+  const uint32_t eb = in_element(args.base, i), ee = in_element(args.exp, i), em = in_element(args.mod, i);
+
+  uint32_t n[L];
+  load_lane_limbs<TPI, L>(n, args.mod.limbs, args.mod.nlimbs, args.mod.stride, em, G.lane);
+  const uint32_t np0 = neg_inv32(G.bcast(n[0], 0));
+
+  const uint32_t W = args.window;
+  uint32_t ebits = exp_bitlen<TPI>(G, args.exp, ee);
+  ebits = __reduce_max_sync(kFull, ebits);
+  const uint32_t nwin = ebits ? (ebits + W - 1) / W : 1;
+
+  uint32_t *slot = args.table + (size_t)(gtid >> 5) * ((size_t)32 * L << W) + (size_t)(threadIdx.x & 31) * L;
+  const size_t entry_stride = (size_t)32 * L;
+
+  uint32_t x[L], t[L], acc[L];
+  // T[0] = R - N, a representative of Mont(1) below R
+#pragma unroll
+  for (int k = 0; k < L; k++) acc[k] = 0;
+  dsub<TPI, L>(G, acc, n, kFull);
+  slot_store<L>(slot, acc);
+  {
+    uint32_t r2[L];
+    compute_r2<TPI, L>(G, r2, n, np0);
+    load_lane_limbs<TPI, L>(x, args.base.limbs, args.base.nlimbs, args.base.stride, eb, G.lane);
+    mont_mul<TPI, L>(G, t, x, r2, n, np0);  // T[1] = Mont(x)
+  }
+  slot_store<L>(slot + entry_stride, t);
+#pragma unroll
+  for (int k = 0; k < L; k++) acc[k] = t[k];
+  const uint32_t entries = 1u << W;
+#pragma unroll 1
+  for (uint32_t e = 2; e < entries; e++) {
+    mont_mul<TPI, L>(G, x, acc, t, n, np0);
+#pragma unroll
+    for (int k = 0; k < L; k++) acc[k] = x[k];
+    slot_store<L>(slot + e * entry_stride, acc);
+  }
+
+  // Main loop: acc holds the running power in Montgomery form.
+  uint32_t win = exp_window(args.exp, ee, (nwin - 1) * W, W);
+  slot_load<L>(slot + win * entry_stride, acc);
+#pragma unroll 1
+  for (int32_t wi = (int32_t)nwin - 2; wi >= 0; wi--) {
+    win = exp_window(args.exp, ee, (uint32_t)wi * W, W);
+    uint32_t y[L];
+    slot_load<L>(slot + win * entry_stride, y);
+#pragma unroll 1
+    for (uint32_t s = 0; s <= W; s++) {
+      uint32_t bsel[L];
+#pragma unroll
+      for (int k = 0; k < L; k++) bsel[k] = (s < W) ? acc[k] : y[k];
+      mont_mul<TPI, L>(G, x, acc, bsel, n, np0);
+#pragma unroll
+      for (int k = 0; k < L; k++) acc[k] = x[k];
+    }
+  }
+
+  // Leave Montgomery form: acc * 1 * R^-1, then reduce below N.
+#pragma unroll
+  for (int k = 0; k < L; k++) t[k] = (G.lane == 0 && k == 0) ? 1u : 0u;
+  mont_mul<TPI, L>(G, x, acc, t, n, np0);
+  dreduce<TPI, L>(G, x, n);
+
+  if (valid) {
+    uint32_t o = out_element(args.out, i);
+    if (o < args.out.count) store_lane_limbs<TPI, L>(x, args.out.limbs, args.out.nlimbs, args.out.stride, o, G.lane);
+  }
+}
+
+}  // namespace xmpb
