@@ -145,9 +145,14 @@ def test_not_shf(handle, bits_out, bits_a):
     rng = np.random.default_rng(18)
     shifts = rng.integers(-400, 400, size=M).astype(np.int32)
     A, C = handle.integers(bits_a, N, a), handle.integers(bits_out, N)
-    xmp.not_(handle, C, A, N)
-    assert np.array_equal(C.export(), oracle.not_(a, bits_out // 32, N))
-    xmp.shf(handle, C, A, shifts, N)
+    if bits_out >= bits_a:
+        xmp.not_(handle, C, A, N)
+        assert np.array_equal(C.export(), oracle.not_(a, bits_out // 32, N))
+    else:  # not needs an output at least as wide as its input (src/logic.cu:500-501)
+        with pytest.raises(xmp.XmpError) as e:
+            xmp.not_(handle, C, A, N)
+        assert e.value.code == xmp.ERR["xmpErrorInvalidPrecision"]
+    xmp.shf(handle, C, A, shifts, N)  # shf has no precision rule
     assert np.array_equal(C.export(), oracle.shf(a, shifts, bits_out // 32, N))
     if bits_out == bits_a:  # in place
         xmp.shf(handle, A, A, shifts, N)
@@ -287,12 +292,12 @@ def test_error_codes(handle):
         big.destroy()
     finally:
         handle.set_policy(None)
-    # scratch limit too small for any window table
+    # scratch limit too small for any window table (import first: it stages host data through scratch)
+    x = handle.integers(1024, 64, oracle.full_length_odd(1, 64, 32))
     tiny = handle.policy()
     tiny.set_scratch_limit(64)
     handle.set_policy(tiny)
     try:
-        x = handle.integers(1024, 64, oracle.full_length_odd(1, 64, 32))
         with pytest.raises(xmp.XmpError) as e:
             xmp.powm(handle, x, x, x, x, 64)
         assert e.value.code == xmp.ERR["xmpErrorIncreaseScratchLimit"]
