@@ -84,6 +84,7 @@ _SIGS = {
     "xmpIntegersDivModAsync": [_VP, _VP, _VP, _VP, _VP, _U32],
     "xmpIntegersPowm": [_VP, _VP, _VP, _VP, _VP, _U32],
     "xmpIntegersPowmAsync": [_VP, _VP, _VP, _VP, _VP, _U32],
+    "xmpIntegersPowmNoAlloc": [_VP, _VP, _VP, _VP, _VP, _U32, _U32, _U32, _U32],
 }
 for _n in ("Add", "Sub", "Mul", "Div", "Mod", "Ior", "And", "Xor"):
     _SIGS["xmpIntegers" + _n] = [_VP, _VP, _VP, _VP, _U32]
