@@ -85,6 +85,10 @@ _SIGS = {
     "xmpIntegersPowm": [_VP, _VP, _VP, _VP, _VP, _U32],
     "xmpIntegersPowmAsync": [_VP, _VP, _VP, _VP, _VP, _U32],
     "xmpIntegersPowmNoAlloc": [_VP, _VP, _VP, _VP, _VP, _U32, _U32, _U32, _U32],
+    "xmpPowmKernelCount": [ctypes.POINTER(_I32)],
+    "xmpPowmKernelGet": [_I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32)],
+    "xmpPowmGetConfig": [_VP, _U32, _U32, _U32, _VP],
+    "xmpIntegersPowmWithConfigAsync": [_VP, _VP, _VP, _VP, _VP, _U32, _VP],
 }
 for _n in ("Add", "Sub", "Mul", "Div", "Mod", "Ior", "And", "Xor"):
     _SIGS["xmpIntegers" + _n] = [_VP, _VP, _VP, _VP, _U32]
@@ -264,6 +268,39 @@ def not_(h, c, a, count, asynchronous=False):
 def divmod_(h, q, r, a, b, count, asynchronous=False):
     fn = lib().xmpIntegersDivModAsync if asynchronous else lib().xmpIntegersDivMod
     check(fn(h.h, _x(q), _x(r), _x(a), _x(b), count), "xmpIntegersDivMod")
+
+
+class PowmConfig(ctypes.Structure):
+    """xmpPowmConfig_t (include/xmp_b200.h)."""
+    _fields_ = [("distribution", ctypes.c_int32), ("lanes", ctypes.c_int32), ("limbs", ctypes.c_int32),
+                ("window", ctypes.c_int32)]
+
+    def __repr__(self):
+        return "PowmConfig(dist=%d, lanes=%d, limbs=%d, window=%d)" % (self.distribution, self.lanes, self.limbs,
+                                                                        self.window)
+
+
+def powm_kernels():
+    """(lanes, limbs) of every register powm kernel compiled into the library."""
+    n = _I32(0)
+    check(lib().xmpPowmKernelCount(ctypes.byref(n)))
+    out = []
+    for i in range(n.value):
+        a, b = _I32(0), _I32(0)
+        check(lib().xmpPowmKernelGet(i, ctypes.byref(a), ctypes.byref(b)))
+        out.append((a.value, b.value))
+    return out
+
+
+def powm_get_config(h, precision, exp_precision, count):
+    c = PowmConfig()
+    check(lib().xmpPowmGetConfig(h.h, precision, exp_precision, count, ctypes.byref(c)), "xmpPowmGetConfig")
+    return c
+
+
+def powm_with_config(h, out, base, exp, mod_, count, config):
+    check(lib().xmpIntegersPowmWithConfigAsync(h.h, _x(out), _x(base), _x(exp), _x(mod_), count,
+                                               ctypes.byref(config)), "xmpIntegersPowmWithConfigAsync")
 
 
 def powm(h, out, base, exp, mod_, count, asynchronous=False):

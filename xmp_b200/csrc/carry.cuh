@@ -71,6 +71,23 @@ __device__ __forceinline__ uint32_t madc_lo(uint32_t a, uint32_t b, uint32_t c) 
   return r;
 }
 
+// a + carry-in (no carry-out) issued as a multiply-add (a*1 + 0 + CC), so the
+// chain's last step can go to the FMA pipe instead of the integer ALU, which
+// the carry-producing adds keep busy.
+__device__ __forceinline__ uint32_t addc_fma(uint32_t a) {
+  uint32_t r;
+  asm volatile("madc.lo.u32 %0, %1, 1, 0;" : "=r"(r) : "r"(a));
+  return r;
+}
+
+// Full 64-bit product a*b (one wide multiply); no carry flag involved, so the
+// compiler may schedule it freely between carry chains.
+__device__ __forceinline__ uint64_t mul_wide(uint32_t a, uint32_t b) {
+  uint64_t r;
+  asm("mul.wide.u32 %0, %1, %2;" : "=l"(r) : "r"(a), "r"(b));
+  return r;
+}
+
 // -n^{-1} mod 2^32 for odd n by Newton-Hensel lifting: x <- x(2 - n x) doubles
 // the number of correct low bits; n*n == 1 mod 8 gives 3 bits to start.
 __host__ __device__ __forceinline__ uint32_t neg_inv32(uint32_t n) {

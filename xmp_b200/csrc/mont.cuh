@@ -116,25 +116,34 @@ __device__ __forceinline__ uint32_t dnormalize(const Group<TPI> &G, uint32_t (&r
 }
 
 // (r, c0, c1) += a * w, where r has L limbs, c0 is the word above them and
-// c1 the word above c0.  Two carry chains: low halves into r[0..L-1], high
-// halves into r[1..L-1], c0.
+// c1 the word above c0.  Each limb's full 32x32 product is one mul.wide.u32
+// (a single wide multiply on the FMA-heavy pipe; a separate mad.hi costs well
+// over twice a mad.lo there, and a mad.wide with a 32-bit addend costs two
+// FMA-pipe instructions), and the products are independent of each other.
+// Two add chains on the integer ALU pipe fold them in: the low halves into
+// r[0..L-1] (carry into c0, c1), then the high halves into r[1..L-1], c0.
+// The carry-in-only tail steps go to the FMA pipe (addc_fma), which leaves
+// both pipes about equally loaded.
 template <int L>
 __device__ __forceinline__ void mac_row(uint32_t (&r)[L], uint32_t &c0, uint32_t &c1, const uint32_t (&a)[L],
                                         uint32_t w) {
-  r[0] = mad_lo_cc(a[0], w, r[0]);
+  uint64_t p[L];
 #pragma unroll
-  for (int k = 1; k < L; k++) r[k] = madc_lo_cc(a[k], w, r[k]);
+  for (int k = 0; k < L; k++) p[k] = mul_wide(a[k], w);
+  r[0] = add_cc(r[0], (uint32_t)p[0]);
+#pragma unroll
+  for (int k = 1; k < L; k++) r[k] = addc_cc(r[k], (uint32_t)p[k]);
   c0 = addc_cc(c0, 0u);
-  c1 = addc(c1, 0u);
+  c1 = addc_fma(c1);
   if (L > 1) {
-    r[1] = mad_hi_cc(a[0], w, r[1]);
+    r[1] = add_cc(r[1], (uint32_t)(p[0] >> 32));
 #pragma unroll
-    for (int k = 2; k < L; k++) r[k] = madc_hi_cc(a[k - 1], w, r[k]);
-    c0 = madc_hi_cc(a[L - 1], w, c0);
+    for (int k = 2; k < L; k++) r[k] = addc_cc(r[k], (uint32_t)(p[k - 1] >> 32));
+    c0 = addc_cc(c0, (uint32_t)(p[L - 1] >> 32));
   } else {
-    c0 = mad_hi_cc(a[0], w, c0);
+    c0 = add_cc(c0, (uint32_t)(p[0] >> 32));
   }
-  c1 = addc(c1, 0u);
+  c1 = addc_fma(c1);
 }
 
 // r = a * b * R^-1 (mod N), almost reduced (r < R).  a, b < R; r must not alias a or b.
@@ -158,7 +167,7 @@ __device__ __forceinline__ void mont_mul(const Group<TPI> &G, uint32_t (&r)[L], 
 #pragma unroll
       for (int j = 0; j < L - 1; j++) r[j] = r[j + 1];
       r[L - 1] = add_cc(t, c0);
-      c0 = addc(c1, 0u);
+      c0 = addc_fma(c1);
       c1 = 0;
     }
   }

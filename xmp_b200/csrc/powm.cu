@@ -7,6 +7,7 @@
 // otherwise from a register/occupancy heuristic; the reference's static
 // Maxwell/Kepler latency tables (powm.cu:120-236) have no counterpart.
 #include "powm.h"
+#include "../../include/xmp_b200.h"
 #include <algorithm>
 #include <math.h>
 
@@ -133,10 +134,8 @@ xmpError_t powm_run(xmpHandle_t h, const PowmConfig &cfg0, const OutView &out, c
 
 }  // namespace xmpb
 
-extern "C" {
-
-xmpError_t XMPAPI xmpIntegersPowmAsync(xmpHandle_t h, xmpIntegers_t out, const xmpIntegers_t base,
-                                        const xmpIntegers_t exp, const xmpIntegers_t mod, uint32_t count) {
+static xmpError_t powm_entry(xmpHandle_t h, xmpIntegers_t out, xmpIntegers_t base, xmpIntegers_t exp,
+                             xmpIntegers_t mod, uint32_t count, const PowmConfig *forced) {
   if (!h || !out || !base || !exp || !mod) return xmpErrorInvalidParameter;
   int dev = h->device;
   if (out->device != dev || base->device != dev || exp->device != dev || mod->device != dev)
@@ -149,8 +148,13 @@ xmpError_t XMPAPI xmpIntegersPowmAsync(xmpHandle_t h, xmpIntegers_t out, const x
   if (base->precision != out->precision || mod->precision != out->precision) return xmpErrorInvalidPrecision;
 
   PowmConfig cfg;
-  bool tuned = (p->algorithm == xmpAlgorithmDefault) && tuner_lookup_powm(h, mod->nlimbs, exp->precision, count, &cfg);
-  if (!tuned) cfg = powm_default_config(mod->nlimbs, exp->precision, count, p->algorithm, h->sm_count);
+  if (forced) {
+    cfg = *forced;
+  } else {
+    bool tuned = (p->algorithm == xmpAlgorithmDefault) &&
+                 tuner_lookup_powm(h, mod->nlimbs, exp->precision, count, &cfg);
+    if (!tuned) cfg = powm_default_config(mod->nlimbs, exp->precision, count, p->algorithm, h->sm_count);
+  }
   if (!powm_config_valid(cfg, mod->nlimbs)) return xmpErrorUnsupported;
 
   bool aliased = (out == base || out == exp || out == mod);
@@ -167,6 +171,13 @@ xmpError_t XMPAPI xmpIntegersPowmAsync(xmpHandle_t h, xmpIntegers_t out, const x
   return check_cuda();
 }
 
+extern "C" {
+
+xmpError_t XMPAPI xmpIntegersPowmAsync(xmpHandle_t h, xmpIntegers_t out, const xmpIntegers_t base,
+                                        const xmpIntegers_t exp, const xmpIntegers_t mod, uint32_t count) {
+  return powm_entry(h, out, base, exp, mod, count, nullptr);
+}
+
 xmpError_t XMPAPI xmpIntegersPowm(xmpHandle_t h, xmpIntegers_t out, const xmpIntegers_t base, const xmpIntegers_t exp,
                                    const xmpIntegers_t mod, uint32_t count) {
   xmpError_t e = xmpIntegersPowmAsync(h, out, base, exp, mod, count);
@@ -174,6 +185,47 @@ xmpError_t XMPAPI xmpIntegersPowm(xmpHandle_t h, xmpIntegers_t out, const xmpInt
   DeviceGuard guard(h->device);
   cudaStreamSynchronize(h->stream);
   return check_cuda();
+}
+
+xmpError_t XMPAPI xmpIntegersPowmWithConfigAsync(xmpHandle_t h, xmpIntegers_t out, const xmpIntegers_t base,
+                                                  const xmpIntegers_t exp, const xmpIntegers_t mod, uint32_t count,
+                                                  const xmpPowmConfig_t *config) {
+  if (!config) return xmpErrorInvalidParameter;
+  PowmConfig c;
+  c.dist = config->distribution;
+  c.tpi = config->lanes;
+  c.limbs = config->limbs;
+  c.window = config->window;
+  if (c.dist != kDistLanes && c.dist != kDistDigit) return xmpErrorInvalidParameter;
+  return powm_entry(h, out, base, exp, mod, count, &c);
+}
+
+xmpError_t XMPAPI xmpPowmKernelCount(int32_t *count) {
+  if (!count) return xmpErrorInvalidParameter;
+  *count = (int32_t)powm_registry().size();
+  return xmpErrorSuccess;
+}
+
+xmpError_t XMPAPI xmpPowmKernelGet(int32_t index, int32_t *lanes, int32_t *limbs) {
+  if (index < 0 || index >= (int32_t)powm_registry().size() || !lanes || !limbs) return xmpErrorInvalidParameter;
+  *lanes = powm_registry()[index].tpi;
+  *limbs = powm_registry()[index].limbs;
+  return xmpErrorSuccess;
+}
+
+xmpError_t XMPAPI xmpPowmGetConfig(xmpHandle_t h, uint32_t precision, uint32_t exp_precision, uint32_t count,
+                                   xmpPowmConfig_t *config) {
+  if (!h || !config || precision == 0 || precision % 32 || exp_precision == 0 || exp_precision % 32)
+    return xmpErrorInvalidParameter;
+  PowmConfig c;
+  bool tuned = (h->policy->algorithm == xmpAlgorithmDefault) &&
+               tuner_lookup_powm(h, precision / 32, exp_precision, count, &c);
+  if (!tuned) c = powm_default_config(precision / 32, exp_precision, count, h->policy->algorithm, h->sm_count);
+  config->distribution = c.dist;
+  config->lanes = c.tpi;
+  config->limbs = c.limbs;
+  config->window = c.window;
+  return xmpErrorSuccess;
 }
 
 }  // extern "C"
