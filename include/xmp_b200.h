@@ -44,6 +44,110 @@ xmpError_t XMPAPI xmpIntegersPowmWithConfigAsync(xmpHandle_t handle, xmpIntegers
                                                   const xmpIntegers_t exp, const xmpIntegers_t mod, uint32_t count,
                                                   const xmpPowmConfig_t *config);
 
+/* ---- batched powm over mixed precisions ------------------------------------
+ * A plan takes plain items (out = base^exp mod mod for `count` instances of
+ * one precision) and CRT items (out = c^d mod pq from the half-size key
+ * material: cp = c mod p, cq = c mod q, mp = cp^dp mod p, mq = cq^dq mod q,
+ * out = mq + q * ((mp - mq) * qinv mod p), Garner recombination; p and q
+ * have their top bit set).  Instances are binned by modulus precision (CRT
+ * halves join the bin of their precision); every bin runs as one persistent
+ * kernel whose warps pull work from an atomic queue, with its configuration
+ * from the handle's tuner, and all bins run concurrently (forked onto side
+ * streams and joined back to the handle's stream).  With `use_graph` the
+ * whole execution is captured once into a CUDA graph and each execute is one
+ * graph launch.  All device memory a plan needs (window tables, CRT
+ * temporaries) is allocated when it is created.  Index policies do not apply;
+ * no item's output may alias another item's input; the arrays must outlive
+ * the plan. */
+typedef struct {
+  xmpIntegers_t out, base, exp, mod;
+  uint32_t count;
+} xmpPowmBatchItem_t;
+
+typedef struct {
+  xmpIntegers_t out;              /* 2h bits */
+  xmpIntegers_t c;                /* 2h bits, c < pq */
+  xmpIntegers_t p, q, dp, dq, qinv; /* h bits */
+  uint32_t count;
+} xmpPowmCRTItem_t;
+
+typedef struct _xmpPowmBatchPlan_t *xmpPowmBatchPlan_t;
+
+xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t handle, const xmpPowmBatchItem_t *items, int32_t n_items,
+                                         const xmpPowmCRTItem_t *crt, int32_t n_crt, int32_t use_graph,
+                                         xmpPowmBatchPlan_t *plan);
+/* Enqueues one execution on the handle's stream. */
+xmpError_t XMPAPI xmpPowmBatchPlanExecute(xmpHandle_t handle, xmpPowmBatchPlan_t plan);
+xmpError_t XMPAPI xmpPowmBatchPlanDestroy(xmpHandle_t handle, xmpPowmBatchPlan_t plan);
+/* Number of bins (concurrent persistent kernels) and each bin's precision, instances and configuration. */
+xmpError_t XMPAPI xmpPowmBatchPlanInfo(xmpPowmBatchPlan_t plan, int32_t *bins, uint32_t *precision, uint32_t *count,
+                                       xmpPowmConfig_t *config, int32_t *blocks, int32_t max_bins);
+
+/* ---- autotuner --------------------------------------------------------------
+ * A problem shape is (op, bits, exp_bits, count).  Each op has candidate
+ * kernel configurations in XMP_TUNE_CANDIDATES slots:
+ *   powm:   slot = 6*d + (W-1), d in {per-thread, 2, 4, 8, 16, 32 lanes,
+ *           digit-serial}, W = window bits 1..6 (42 slots; each lane count uses
+ *           the fewest limbs per lane that hold the precision);
+ *   mul, divmod: slot = 4*v + t, v in {register kernel, streamed kernel},
+ *           t -> 32, 64, 128, 256 threads per block (8 slots).
+ * Slots a shape cannot use are invalid. */
+enum { xmpTuneMul = 0, xmpTuneDivMod = 1, xmpTunePowm = 2 };
+#define XMP_TUNE_CANDIDATES 48
+
+typedef struct {
+  int32_t op;        /* xmpTuneMul, xmpTuneDivMod, xmpTunePowm */
+  uint32_t bits;     /* modulus / operand precision (divmod: dividend = 2*bits, divisor = bits) */
+  uint32_t exp_bits; /* powm exponent length in bits (0 otherwise) */
+  uint32_t count;    /* instances */
+} xmpTuneShape_t;
+
+/* Whether `slot` is a valid candidate for (op, bits) and the configuration it
+ * stands for (powm: all four fields; mul/divmod: distribution = 0 register /
+ * 1 streamed, lanes = threads per block). */
+xmpError_t XMPAPI xmpTuneCandidate(int32_t op, uint32_t bits, int32_t slot, int32_t *valid,
+                                   xmpPowmConfig_t *config);
+
+/* Exhaustive tuner: times every valid candidate of `shape` on seeded synthetic
+ * data (CUDA events on the handle's stream, best of `reps`); ms[slot] is the
+ * time in milliseconds, a negative value for invalid slots, or NaN for valid
+ * slots of a distribution whose first timing was already over 20x the best
+ * (not worth timing its other windows). */
+xmpError_t XMPAPI xmpTuneMeasure(xmpHandle_t handle, const xmpTuneShape_t *shape, int32_t reps, float *ms);
+
+/* Records / queries the handle's choice for a shape.  Lookup order: a choice
+ * set for the exact shape, else the loaded selector's table, else the
+ * built-in heuristic (source 1, 2, 0). */
+xmpError_t XMPAPI xmpTuneSetChoice(xmpHandle_t handle, const xmpTuneShape_t *shape, int32_t slot);
+xmpError_t XMPAPI xmpTuneGetChoice(xmpHandle_t handle, const xmpTuneShape_t *shape, int32_t *slot, int32_t *source);
+xmpError_t XMPAPI xmpTuneClear(xmpHandle_t handle);
+
+/* ---- learned selector ------------------------------------------------------
+ * MLP with 4 inputs (op, log2 bits, log2 count, log2 exp_bits, scaled), two
+ * hidden layers of 64 FP32 ReLU units and one predicted log2(time) per
+ * candidate slot.  Parameters are XMP_SELECTOR_PARAMS floats laid out as
+ * W1[4][64], b1[64], W2[64][64], b2[64], W3[64][48], b3[48].  Training,
+ * gradients and inference run in this library's own CUDA kernels. */
+#define XMP_SELECTOR_HIDDEN 64
+#define XMP_SELECTOR_PARAMS (4 * 64 + 64 + 64 * 64 + 64 + 64 * 48 + 48)
+
+/* Trains from measured times ms[n][48] (negative = invalid) with Adam for
+ * `epochs` full-batch steps; params is read as the initial value when
+ * `init_from_params` is nonzero, else initialised from `seed`; final loss out. */
+xmpError_t XMPAPI xmpSelectorTrain(xmpHandle_t handle, const xmpTuneShape_t *shapes, const float *ms, int32_t n,
+                                   int32_t epochs, float learning_rate, uint64_t seed, int32_t init_from_params,
+                                   float *params, float *final_loss);
+/* Loss and its gradient with respect to every parameter (for checking). */
+xmpError_t XMPAPI xmpSelectorGradients(xmpHandle_t handle, const float *params, const xmpTuneShape_t *shapes,
+                                       const float *ms, int32_t n, float *loss, float *grads);
+/* Predicted log2(ms) for every slot of n shapes (pred[n][48]). */
+xmpError_t XMPAPI xmpSelectorPredict(xmpHandle_t handle, const float *params, const xmpTuneShape_t *shapes,
+                                     int32_t n, float *pred);
+/* Installs a trained selector in the handle: a CUDA kernel evaluates it over
+ * the lookup grid (every 32-bit precision up to 16,384 bits x log2 count x
+ * log2 exponent length) and the per-call choice becomes a table lookup. */
+xmpError_t XMPAPI xmpSelectorLoad(xmpHandle_t handle, const float *params);
+
 #ifdef __cplusplus
 }
 #endif

@@ -89,6 +89,19 @@ _SIGS = {
     "xmpPowmKernelGet": [_I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32)],
     "xmpPowmGetConfig": [_VP, _U32, _U32, _U32, _VP],
     "xmpIntegersPowmWithConfigAsync": [_VP, _VP, _VP, _VP, _VP, _U32, _VP],
+    "xmpTuneCandidate": [_I32, _U32, _I32, ctypes.POINTER(_I32), _VP],
+    "xmpTuneMeasure": [_VP, _VP, _I32, _VP],
+    "xmpTuneSetChoice": [_VP, _VP, _I32],
+    "xmpTuneGetChoice": [_VP, _VP, ctypes.POINTER(_I32), ctypes.POINTER(_I32)],
+    "xmpTuneClear": [_VP],
+    "xmpSelectorTrain": [_VP, _VP, _VP, _I32, _I32, ctypes.c_float, ctypes.c_uint64, _I32, _VP, _VP],
+    "xmpSelectorGradients": [_VP, _VP, _VP, _VP, _I32, _VP, _VP],
+    "xmpSelectorPredict": [_VP, _VP, _VP, _I32, _VP],
+    "xmpSelectorLoad": [_VP, _VP],
+    "xmpPowmBatchPlanCreate": [_VP, _VP, _I32, _VP, _I32, _I32, ctypes.POINTER(_VP)],
+    "xmpPowmBatchPlanExecute": [_VP, _VP],
+    "xmpPowmBatchPlanDestroy": [_VP, _VP],
+    "xmpPowmBatchPlanInfo": [_VP, ctypes.POINTER(_I32), _VP, _VP, _VP, _VP, _I32],
 }
 for _n in ("Add", "Sub", "Mul", "Div", "Mod", "Ior", "And", "Xor"):
     _SIGS["xmpIntegers" + _n] = [_VP, _VP, _VP, _VP, _U32]
@@ -301,6 +314,47 @@ def powm_get_config(h, precision, exp_precision, count):
 def powm_with_config(h, out, base, exp, mod_, count, config):
     check(lib().xmpIntegersPowmWithConfigAsync(h.h, _x(out), _x(base), _x(exp), _x(mod_), count,
                                                ctypes.byref(config)), "xmpIntegersPowmWithConfigAsync")
+
+
+class BatchItem(ctypes.Structure):
+    """xmpPowmBatchItem_t: out = base^exp mod mod for `count` instances."""
+    _fields_ = [("out", _VP), ("base", _VP), ("exp", _VP), ("mod", _VP), ("count", _U32)]
+
+
+class CRTItem(ctypes.Structure):
+    """xmpPowmCRTItem_t: out = c^d mod pq from (p, q, dp, dq, qinv)."""
+    _fields_ = [("out", _VP), ("c", _VP), ("p", _VP), ("q", _VP), ("dp", _VP), ("dq", _VP), ("qinv", _VP),
+                ("count", _U32)]
+
+
+class BatchPlan:
+    """A batched mixed-precision powm plan (xmpPowmBatchPlan_t)."""
+
+    def __init__(self, h, items=(), crt=(), use_graph=True):
+        self.h = h
+        it = (BatchItem * max(1, len(items)))(*[BatchItem(_x(o), _x(b), _x(e), _x(m), c) for o, b, e, m, c in items])
+        cr = (CRTItem * max(1, len(crt)))(*[CRTItem(*[_x(v) for v in row[:7]], row[7]) for row in crt])
+        p = _VP()
+        check(lib().xmpPowmBatchPlanCreate(h.h, it, len(items), cr, len(crt), 1 if use_graph else 0, ctypes.byref(p)),
+              "xmpPowmBatchPlanCreate")
+        self.p = p
+
+    def execute(self):
+        check(lib().xmpPowmBatchPlanExecute(self.h.h, self.p), "xmpPowmBatchPlanExecute")
+
+    def info(self):
+        n = _I32(0)
+        prec = (_U32 * 64)()
+        cnt = (_U32 * 64)()
+        cfg = (PowmConfig * 64)()
+        blk = (_I32 * 64)()
+        check(lib().xmpPowmBatchPlanInfo(self.p, ctypes.byref(n), prec, cnt, cfg, blk, 64))
+        return [dict(precision=prec[i], count=cnt[i], config=cfg[i], blocks=blk[i]) for i in range(n.value)]
+
+    def destroy(self):
+        if self.p:
+            check(lib().xmpPowmBatchPlanDestroy(self.h.h, self.p), "xmpPowmBatchPlanDestroy")
+            self.p = None
 
 
 def powm(h, out, base, exp, mod_, count, asynchronous=False):

@@ -21,6 +21,7 @@
 // window and divisor in the scratch arena.
 #include "internal.h"
 #include "carry.cuh"
+#include "tune.h"
 #include <algorithm>
 
 using namespace xmpb;
@@ -131,7 +132,7 @@ __device__ __forceinline__ bool div_trivial(const DivArgs &d, uint32_t ea, uint3
 }
 
 template <int BN>
-__global__ void __launch_bounds__(128) divmod_reg_kernel(DivArgs d) {
+__global__ void __launch_bounds__(256) divmod_reg_kernel(DivArgs d) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.count) return;
   const uint32_t ea = in_element(d.a, i), eb = in_element(d.b, i);
@@ -204,7 +205,7 @@ __global__ void __launch_bounds__(128) divmod_reg_kernel(DivArgs d) {
 }
 
 // Same algorithm with the window and divisor in scratch (any divisor size).
-__global__ void __launch_bounds__(128) divmod_stream_kernel(DivArgs d) {
+__global__ void __launch_bounds__(256) divmod_stream_kernel(DivArgs d) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.count) return;
   const uint32_t ea = in_element(d.a, i), eb = in_element(d.b, i);
@@ -275,10 +276,10 @@ __global__ void __launch_bounds__(128) divmod_stream_kernel(DivArgs d) {
   }
 }
 
-typedef void (*DivLaunch)(const DivArgs &, cudaStream_t);
+typedef void (*DivLaunch)(const DivArgs &, int, cudaStream_t);
 template <int BN>
-static void launch_div(const DivArgs &d, cudaStream_t s) {
-  divmod_reg_kernel<BN><<<grid_for(d.count, 128), 128, 0, s>>>(d);
+static void launch_div(const DivArgs &d, int threads, cudaStream_t s) {
+  divmod_reg_kernel<BN><<<grid_for(d.count, threads), threads, 0, s>>>(d);
 }
 static DivLaunch pick_div(uint32_t nb) {
   if (nb <= 1) return launch_div<1>;
@@ -295,8 +296,10 @@ static DivLaunch pick_div(uint32_t nb) {
   return nullptr;
 }
 
+bool div_has_register_kernel(uint32_t nb) { return pick_div(nb) != nullptr; }
+
 static xmpError_t divmod_common(xmpHandle_t h, xmpIntegers_t q, xmpIntegers_t r, xmpIntegers_t a, xmpIntegers_t b,
-                                uint32_t count, int qi, int ri, int ai, int bi) {
+                                uint32_t count, int qi, int ri, int ai, int bi, const ElemConfig *forced) {
   xmpExecutionPolicy_t pol = h->policy;
   DivArgs d;
   d.a = view_in(a, pol->indices[ai], pol->indices_count[ai]);
@@ -306,6 +309,17 @@ static xmpError_t divmod_common(xmpHandle_t h, xmpIntegers_t q, xmpIntegers_t r,
   d.T = 0;
   DivLaunch launch = pol->algorithm == xmpAlgorithmDigitMP ? nullptr : pick_div(b->nlimbs);
   if (pol->algorithm == xmpAlgorithmRegMP && !launch) return xmpErrorUnsupported;
+  ElemConfig cfg;
+  if (forced) {
+    cfg = *forced;
+  } else if (pol->algorithm == xmpAlgorithmDefault) {
+    int slot = tuner_lookup(h, xmpTuneDivMod, b->precision, 0, count, nullptr);
+    ElemConfig t;
+    if (slot >= 0 && elem_candidate(xmpTuneDivMod, b->nlimbs, slot, &t)) cfg = t;
+  }
+  if (cfg.variant == 1) launch = nullptr;
+  else if (!launch && forced) return xmpErrorUnsupported;
+  const int threads = cfg.threads;
 
   OutTarget tq, tr;
   xmpError_t e;
@@ -329,13 +343,13 @@ static xmpError_t divmod_common(xmpHandle_t h, xmpIntegers_t q, xmpIntegers_t r,
   d.q = q ? view_out(q, tq.limbs, qi >= 0 ? pol->indices[qi] : nullptr) : OutView{nullptr, 0, 0, 0, nullptr};
   d.r = r ? view_out(r, tr.limbs, ri >= 0 ? pol->indices[ri] : nullptr) : OutView{nullptr, 0, 0, 0, nullptr};
   if (launch) {
-    launch(d, h->stream);
+    launch(d, threads, h->stream);
   } else {
-    d.T = round_up(count, 128);
+    d.T = round_up(count, 256);
     e = ensure_scratch(h, (size_t)(2 * b->nlimbs + 1) * d.T * 4);
     if (e != xmpErrorSuccess) return e;
     d.scratch = (uint32_t *)h->scratch;
-    divmod_stream_kernel<<<grid_for(count, 128), 128, 0, h->stream>>>(d);
+    divmod_stream_kernel<<<grid_for(count, threads), threads, 0, h->stream>>>(d);
   }
   if (q) {
     e = end_output(h, q, tq);
@@ -346,6 +360,22 @@ static xmpError_t divmod_common(xmpHandle_t h, xmpIntegers_t q, xmpIntegers_t r,
     if (e != xmpErrorSuccess) return e;
   }
   return check_cuda();
+}
+
+xmpError_t divmod_entry(xmpHandle_t h, xmpIntegers_t q, xmpIntegers_t r, xmpIntegers_t a, xmpIntegers_t b,
+                        uint32_t count, const ElemConfig *forced) {
+  if (!h || !q || !r || !a || !b) return xmpErrorInvalidParameter;
+  int dev = h->device;
+  if (q->device != dev || r->device != dev || a->device != dev || b->device != dev) return xmpErrorInvalidDevice;
+  if (count == 0) return xmpErrorSuccess;
+  DeviceGuard guard(dev);
+  xmpExecutionPolicy_t p = h->policy;
+  if (r->count < count || q->count < count) return xmpErrorInvalidCount;
+  if (p->indices[0] && p->indices_count[0] < count) return xmpErrorInvalidCount;
+  if (p->indices[1] && p->indices_count[1] < count) return xmpErrorInvalidCount;
+  if (q->precision < a->precision || r->precision < b->precision) return xmpErrorInvalidPrecision;
+  if (q == r) return xmpErrorInvalidParameter;
+  return divmod_common(h, q, r, a, b, count, 0, 1, 2, 3, forced);
 }
 
 static xmpError_t sync_after(xmpHandle_t h, xmpError_t e) {
@@ -369,7 +399,7 @@ xmpError_t XMPAPI xmpIntegersDivAsync(xmpHandle_t h, xmpIntegers_t q, const xmpI
   if (q->count < count) return xmpErrorInvalidCount;
   if (p->indices[0] && p->indices_count[0] < count) return xmpErrorInvalidCount;
   if (q->precision < a->precision) return xmpErrorInvalidPrecision;
-  return divmod_common(h, q, nullptr, a, b, count, 0, -1, 1, 2);
+  return divmod_common(h, q, nullptr, a, b, count, 0, -1, 1, 2, nullptr);
 }
 xmpError_t XMPAPI xmpIntegersDiv(xmpHandle_t h, xmpIntegers_t q, const xmpIntegers_t a, const xmpIntegers_t b,
                                   uint32_t count) {
@@ -386,7 +416,7 @@ xmpError_t XMPAPI xmpIntegersModAsync(xmpHandle_t h, xmpIntegers_t m, const xmpI
   if (m->count < count) return xmpErrorInvalidCount;
   if (p->indices[0] && p->indices_count[0] < count) return xmpErrorInvalidCount;
   if (m->precision < b->precision) return xmpErrorInvalidPrecision;
-  return divmod_common(h, nullptr, m, a, b, count, -1, 0, 1, 2);
+  return divmod_common(h, nullptr, m, a, b, count, -1, 0, 1, 2, nullptr);
 }
 xmpError_t XMPAPI xmpIntegersMod(xmpHandle_t h, xmpIntegers_t m, const xmpIntegers_t a, const xmpIntegers_t b,
                                   uint32_t count) {
@@ -395,18 +425,7 @@ xmpError_t XMPAPI xmpIntegersMod(xmpHandle_t h, xmpIntegers_t m, const xmpIntege
 
 xmpError_t XMPAPI xmpIntegersDivModAsync(xmpHandle_t h, xmpIntegers_t q, xmpIntegers_t m, const xmpIntegers_t a,
                                           const xmpIntegers_t b, uint32_t count) {
-  if (!h || !q || !m || !a || !b) return xmpErrorInvalidParameter;
-  int dev = h->device;
-  if (q->device != dev || m->device != dev || a->device != dev || b->device != dev) return xmpErrorInvalidDevice;
-  if (count == 0) return xmpErrorSuccess;
-  DeviceGuard guard(dev);
-  xmpExecutionPolicy_t p = h->policy;
-  if (m->count < count || q->count < count) return xmpErrorInvalidCount;
-  if (p->indices[0] && p->indices_count[0] < count) return xmpErrorInvalidCount;
-  if (p->indices[1] && p->indices_count[1] < count) return xmpErrorInvalidCount;
-  if (q->precision < a->precision || m->precision < b->precision) return xmpErrorInvalidPrecision;
-  if (q == m) return xmpErrorInvalidParameter;
-  return divmod_common(h, q, m, a, b, count, 0, 1, 2, 3);
+  return divmod_entry(h, q, m, a, b, count, nullptr);
 }
 xmpError_t XMPAPI xmpIntegersDivMod(xmpHandle_t h, xmpIntegers_t q, xmpIntegers_t m, const xmpIntegers_t a,
                                      const xmpIntegers_t b, uint32_t count) {

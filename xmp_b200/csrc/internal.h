@@ -26,22 +26,22 @@ __host__ __device__ inline uint32_t round_up(uint32_t n, uint32_t d) { return di
 
 // Read-only description of one operand as seen by a kernel.
 struct ArrayView {
-  uint32_t *limbs;    // interleaved storage
-  uint32_t nlimbs;    // precision / 32
-  uint32_t stride;    // instances per limb-group row
-  uint32_t count;     // array count (for broadcast modulo)
-  const uint32_t *index;  // optional gather index array (device)
-  uint32_t index_count;
+  uint32_t *limbs = nullptr;    // interleaved storage
+  uint32_t nlimbs = 0;          // precision / 32
+  uint32_t stride = 0;          // instances per limb-group row
+  uint32_t count = 0;           // array count (for broadcast modulo)
+  const uint32_t *index = nullptr;  // optional gather index array (device)
+  uint32_t index_count = 0;
 };
 
 // Output description: scatter index is out_index[i] (no modulo), as in the
 // reference kernels (implementations.h:66).
 struct OutView {
-  uint32_t *limbs;
-  uint32_t nlimbs;
-  uint32_t stride;
-  uint32_t count;         // writes to elements >= count are dropped (bad scatter index)
-  const uint32_t *index;
+  uint32_t *limbs = nullptr;
+  uint32_t nlimbs = 0;
+  uint32_t stride = 0;
+  uint32_t count = 0;     // writes to elements >= count are dropped (bad scatter index)
+  const uint32_t *index = nullptr;
 };
 
 // Input element selected by op instance i (docs 15-16; implementations.h:63-68).

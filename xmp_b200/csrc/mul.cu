@@ -13,6 +13,7 @@
 // kernels.
 #include "internal.h"
 #include "carry.cuh"
+#include "tune.h"
 #include <algorithm>
 
 using namespace xmpb;
@@ -47,7 +48,7 @@ __device__ __forceinline__ void store_limbs(const uint32_t (&x)[N], const OutVie
 }
 
 template <int AL, int BL>
-__global__ void __launch_bounds__(128) mul_reg_kernel(ArrayView a, ArrayView b, OutView c, uint32_t count) {
+__global__ void __launch_bounds__(256) mul_reg_kernel(ArrayView a, ArrayView b, OutView c, uint32_t count) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   uint32_t ea = in_element(a, i), eb = in_element(b, i), ec = out_element(c, i);
@@ -73,7 +74,7 @@ __global__ void __launch_bounds__(128) mul_reg_kernel(ArrayView a, ArrayView b, 
 }
 
 // Column k of the product, accumulated from the interleaved arrays.
-__global__ void __launch_bounds__(128) mul_stream_kernel(ArrayView a, ArrayView b, OutView c, uint32_t count) {
+__global__ void __launch_bounds__(256) mul_stream_kernel(ArrayView a, ArrayView b, OutView c, uint32_t count) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   uint32_t ea = in_element(a, i), eb = in_element(b, i), ec = out_element(c, i);
@@ -102,10 +103,10 @@ __global__ void __launch_bounds__(128) mul_stream_kernel(ArrayView a, ArrayView 
   }
 }
 
-typedef void (*MulLaunch)(ArrayView, ArrayView, OutView, uint32_t, cudaStream_t);
+typedef void (*MulLaunch)(ArrayView, ArrayView, OutView, uint32_t, int, cudaStream_t);
 template <int AL, int BL>
-static void launch_mul(ArrayView a, ArrayView b, OutView c, uint32_t count, cudaStream_t s) {
-  mul_reg_kernel<AL, BL><<<grid_for(count, 128), 128, 0, s>>>(a, b, c, count);
+static void launch_mul(ArrayView a, ArrayView b, OutView c, uint32_t count, int threads, cudaStream_t s) {
+  mul_reg_kernel<AL, BL><<<grid_for(count, threads), threads, 0, s>>>(a, b, c, count);
 }
 
 static const int kClasses[] = {2, 4, 8, 12, 16, 24, 32};
@@ -127,12 +128,15 @@ static MulLaunch pick_mul(int al, int bl) {
   return nullptr;
 }
 
-}  // namespace xmpb
+bool mul_has_register_kernel(uint32_t na, uint32_t nb) {
+  int al = class_of(std::max(na, nb)), bl = class_of(std::min(na, nb));
+  return al && bl && pick_mul(al, bl) != nullptr;
+}
 
-extern "C" {
-
-xmpError_t XMPAPI xmpIntegersMulAsync(xmpHandle_t h, xmpIntegers_t p, const xmpIntegers_t a, const xmpIntegers_t b,
-                                       uint32_t count) {
+// Register kernel when one exists for the operand classes (else the streamed
+// kernel), 128 threads -- unless the tuner or the caller chose otherwise.
+xmpError_t mul_entry(xmpHandle_t h, xmpIntegers_t p, xmpIntegers_t a, xmpIntegers_t b, uint32_t count,
+                     const ElemConfig *forced) {
   if (!h || !p || !a || !b) return xmpErrorInvalidParameter;
   int dev = h->device;
   if (p->device != dev || a->device != dev || b->device != dev) return xmpErrorInvalidDevice;
@@ -151,6 +155,17 @@ xmpError_t XMPAPI xmpIntegersMulAsync(xmpHandle_t h, xmpIntegers_t p, const xmpI
   MulLaunch launch = nullptr;
   if (al && bl && pol->algorithm != xmpAlgorithmDigitMP) launch = pick_mul(al, bl);
   if (pol->algorithm == xmpAlgorithmRegMP && !launch) return xmpErrorUnsupported;
+  ElemConfig cfg;
+  if (forced) {
+    cfg = *forced;
+  } else if (pol->algorithm == xmpAlgorithmDefault) {
+    int slot = tuner_lookup(h, xmpTuneMul, std::max(a->precision, b->precision), 0, count, nullptr);
+    ElemConfig t;
+    if (slot >= 0 && elem_candidate(xmpTuneMul, std::max(a->nlimbs, b->nlimbs), slot, &t)) cfg = t;
+  }
+  if (cfg.variant == 1) launch = nullptr;
+  else if (!launch && forced) return xmpErrorUnsupported;
+  const int threads = cfg.threads;
   bool aliased = (p == a || p == b);
   bool indexed = pol->indices[0] || pol->indices[1] || pol->indices[2];
   OutTarget t;
@@ -159,12 +174,21 @@ xmpError_t XMPAPI xmpIntegersMulAsync(xmpHandle_t h, xmpIntegers_t p, const xmpI
   if (e != xmpErrorSuccess) return e;
   OutView vc = view_out(p, t.limbs, pol->indices[0]);
   if (launch)
-    launch(va, vb, vc, count, h->stream);
+    launch(va, vb, vc, count, threads, h->stream);
   else
-    mul_stream_kernel<<<grid_for(count, 128), 128, 0, h->stream>>>(va, vb, vc, count);
+    mul_stream_kernel<<<grid_for(count, threads), threads, 0, h->stream>>>(va, vb, vc, count);
   e = end_output(h, p, t);
   if (e != xmpErrorSuccess) return e;
   return check_cuda();
+}
+
+}  // namespace xmpb
+
+extern "C" {
+
+xmpError_t XMPAPI xmpIntegersMulAsync(xmpHandle_t h, xmpIntegers_t p, const xmpIntegers_t a, const xmpIntegers_t b,
+                                       uint32_t count) {
+  return mul_entry(h, p, a, b, count, nullptr);
 }
 
 xmpError_t XMPAPI xmpIntegersMul(xmpHandle_t h, xmpIntegers_t p, const xmpIntegers_t a, const xmpIntegers_t b,

@@ -17,20 +17,25 @@ struct PowmConfig {
 };
 
 typedef void (*PowmLauncher)(const PowmArgs &args, int grid, cudaStream_t stream);
+typedef void (*PowmBatchLauncher)(const PowmBatchArgs &args, int grid, cudaStream_t stream);
 
 struct PowmKernelEntry {
   int tpi;
   int limbs;
   PowmLauncher launch;
   const void *fn;
+  PowmBatchLauncher launch_batch;
+  const void *batch_fn;
+  PowmLauncher launch_r2;
 };
 
 std::vector<PowmKernelEntry> &powm_registry();
 const PowmKernelEntry *powm_find(int tpi, int limbs);
 
 struct PowmKernelRegistrar {
-  PowmKernelRegistrar(int tpi, int limbs, PowmLauncher l, const void *fn) {
-    powm_registry().push_back(PowmKernelEntry{tpi, limbs, l, fn});
+  PowmKernelRegistrar(int tpi, int limbs, PowmLauncher l, const void *fn, PowmBatchLauncher lb, const void *bfn,
+                      PowmLauncher lr2) {
+    powm_registry().push_back(PowmKernelEntry{tpi, limbs, l, fn, lb, bfn, lr2});
   }
 };
 
@@ -38,8 +43,17 @@ struct PowmKernelRegistrar {
   static void powm_launch_##TPI##_##L(const PowmArgs &a, int grid, cudaStream_t s) {                \
     powm_kernel<TPI, L><<<grid, 128, 0, s>>>(a);                                                     \
   }                                                                                                   \
+  static void powm_launch_batch_##TPI##_##L(const PowmBatchArgs &a, int grid, cudaStream_t s) {     \
+    powm_batch_kernel<TPI, L><<<grid, 128, 0, s>>>(a);                                               \
+  }                                                                                                   \
+  static void powm_launch_r2_##TPI##_##L(const PowmArgs &a, int grid, cudaStream_t s) {             \
+    r2_kernel<TPI, L><<<grid, 128, 0, s>>>(a);                                                       \
+  }                                                                                                   \
   static PowmKernelRegistrar powm_reg_##TPI##_##L(TPI, L, powm_launch_##TPI##_##L,                  \
-                                                  (const void *)powm_kernel<TPI, L>);
+                                                  (const void *)powm_kernel<TPI, L>,                 \
+                                                  powm_launch_batch_##TPI##_##L,                     \
+                                                  (const void *)powm_batch_kernel<TPI, L>,           \
+                                                  powm_launch_r2_##TPI##_##L);
 
 // Best fixed window for a k-bit exponent: minimises table build (2^W - 2
 // multiplies) plus one multiply per window.

@@ -29,6 +29,8 @@ namespace xmpb {
 
 struct PowmArgs {
   ArrayView base, exp, mod;
+  ArrayView r2;     // optional (limbs == nullptr: computed per instance): R^2 mod N per modulus element,
+                    // R = 2^(32 * TPI * L), indexed like `mod`
   OutView out;
   uint32_t start;   // first op instance of this launch
   uint32_t count;   // op instances in this launch
@@ -133,14 +135,12 @@ __device__ __forceinline__ uint32_t exp_bitlen(const Group<TPI> &G, const ArrayV
   return G.seg_max(bl);
 }
 
+// One instance group: op instance i of `args` (every lane of the warp calls
+// this together; `valid` lanes store their result).  `slot` is this lane's
+// window-table slot (entry e at slot + e*32*L).
 template <int TPI, int L>
-__global__ void __launch_bounds__(128) powm_kernel(PowmArgs args) {
-  Group<TPI> G;
-  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t local = gtid / TPI;
-  const bool valid = local < args.count;
-  // Lanes past the end run a copy of the last instance so every shfl sees a full warp.
-  const uint32_t i = args.start + (valid ? local : args.count - 1);
+__device__ __forceinline__ void powm_instance(const Group<TPI> &G, const PowmArgs &args, uint32_t i, bool valid,
+                                              uint32_t *slot) {
   const uint32_t eb = in_element(args.base, i), ee = in_element(args.exp, i), em = in_element(args.mod, i);
 
   uint32_t n[L];
@@ -152,7 +152,6 @@ __global__ void __launch_bounds__(128) powm_kernel(PowmArgs args) {
   ebits = __reduce_max_sync(kFull, ebits);
   const uint32_t nwin = ebits ? (ebits + W - 1) / W : 1;
 
-  uint32_t *slot = args.table + (size_t)(gtid >> 5) * ((size_t)32 * L << W) + (size_t)(threadIdx.x & 31) * L;
   const size_t entry_stride = (size_t)32 * L;
 
   uint32_t x[L], t[L], acc[L];
@@ -163,7 +162,10 @@ __global__ void __launch_bounds__(128) powm_kernel(PowmArgs args) {
   slot_store<L>(slot, acc);
   {
     uint32_t r2[L];
-    compute_r2<TPI, L>(G, r2, n, np0);
+    if (args.r2.limbs)
+      load_lane_limbs<TPI, L>(r2, args.r2.limbs, args.r2.nlimbs, args.r2.stride, in_element(args.r2, i), G.lane);
+    else
+      compute_r2<TPI, L>(G, r2, n, np0);
     load_lane_limbs<TPI, L>(x, args.base.limbs, args.base.nlimbs, args.base.stride, eb, G.lane);
     mont_mul<TPI, L>(G, t, x, r2, n, np0);  // T[1] = Mont(x)
   }
@@ -207,6 +209,78 @@ __global__ void __launch_bounds__(128) powm_kernel(PowmArgs args) {
   if (valid) {
     uint32_t o = out_element(args.out, i);
     if (o < args.out.count) store_lane_limbs<TPI, L>(x, args.out.limbs, args.out.nlimbs, args.out.stride, o, G.lane);
+  }
+}
+
+
+template <int TPI, int L>
+__global__ void __launch_bounds__(128) powm_kernel(PowmArgs args) {
+  Group<TPI> G;
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t local = gtid / TPI;
+  const bool valid = local < args.count;
+  // Lanes past the end run a copy of the last instance so every shfl sees a full warp.
+  const uint32_t i = args.start + (valid ? local : args.count - 1);
+  uint32_t *slot = args.table + (size_t)(gtid >> 5) * ((size_t)32 * L << args.window) + (size_t)(threadIdx.x & 31) * L;
+  powm_instance<TPI, L>(G, args, i, valid, slot);
+}
+
+// R^2 mod N (R = 2^(32 * TPI * L)) for every element of `args.mod`, written
+// to `args.out` (server set-up: Montgomery constants kept on the device).
+template <int TPI, int L>
+__global__ void __launch_bounds__(128) r2_kernel(PowmArgs args) {
+  Group<TPI> G;
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t local = gtid / TPI;
+  const bool valid = local < args.count;
+  const uint32_t i = valid ? local : args.count - 1;
+  uint32_t n[L], r2[L];
+  load_lane_limbs<TPI, L>(n, args.mod.limbs, args.mod.nlimbs, args.mod.stride, i, G.lane);
+  const uint32_t np0 = neg_inv32(G.bcast(n[0], 0));
+  compute_r2<TPI, L>(G, r2, n, np0);
+  // the stored value must be below R and fit the output's limbs: keep it exact (< N)
+  dreduce<TPI, L>(G, r2, n);
+  if (valid) store_lane_limbs<TPI, L>(r2, args.out.limbs, args.out.nlimbs, args.out.stride, i, G.lane);
+}
+
+// Persistent form for batched launches: a fixed grid whose warps pull work
+// items (32/TPI consecutive instances) from an atomic queue over up to
+// kPowmSegs segments (arrays of the same precision, e.g. plain instances and
+// CRT half-exponentiations), so kernels of several precisions can share the
+// GPU for their whole duration.  Only the launched warps need table slots.
+// The queue is one counter word: every warp only ever increments it, so
+// nothing waits on another warp.
+constexpr int kPowmSegs = 4;
+struct PowmBatchArgs {
+  PowmArgs seg[kPowmSegs];  // each seg's start/count select its instances; table is ignored
+  uint32_t nseg;
+  uint32_t items;            // work items in total
+  uint32_t item_start[kPowmSegs + 1];  // prefix sums of items per segment
+  uint32_t window;
+  uint32_t *table;
+  uint32_t *counter;         // zeroed before the launch
+};
+
+template <int TPI, int L>
+__global__ void __launch_bounds__(128) powm_batch_kernel(PowmBatchArgs b) {
+  Group<TPI> G;
+  const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint32_t *slot = b.table + (size_t)gwarp * ((size_t)32 * L << b.window) + (size_t)(threadIdx.x & 31) * L;
+  constexpr uint32_t per_item = 32 / TPI;
+  while (true) {
+    uint32_t item = 0;
+    if ((threadIdx.x & 31) == 0) item = atomicAdd(b.counter, 1u);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= b.items) break;
+    uint32_t s = 0;
+    while (s + 1 < b.nseg && item >= b.item_start[s + 1]) s++;
+    const PowmArgs &a = b.seg[s];
+    const uint32_t local = (item - b.item_start[s]) * per_item + (threadIdx.x & 31) / TPI;
+    const bool valid = local < a.count;
+    const uint32_t i = a.start + (valid ? local : a.count - 1);
+    PowmArgs args = a;
+    args.window = b.window;
+    powm_instance<TPI, L>(G, args, i, valid, slot);
   }
 }
 

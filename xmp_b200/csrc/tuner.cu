@@ -1,10 +1,311 @@
-// Autotuner state attached to a handle (placeholder until the tuner lands).
-#include "powm.h"
+// Runtime autotuner (replaces the reference's offline tuner, src/tune/tune.cu,
+// whose static per-architecture latency tables src/powm.cu:117-236 reads).
+//
+// Candidates per shape are enumerated by slot (see include/xmp_b200.h); the
+// exhaustive tuner times every valid one on seeded synthetic data generated
+// on the device, with CUDA events on the handle's stream.  Choices live in a
+// per-handle table: exact shapes set by the tuner first, then the learned
+// selector's dense grid, then the built-in heuristic.
+#include "tune.h"
+#include <algorithm>
+#include <math.h>
+
+using namespace xmpb;
 
 namespace xmpb {
-bool tuner_lookup_powm(xmpHandle_t h, uint32_t nlimbs, uint32_t exp_bits, uint32_t count, PowmConfig *cfg) {
-  (void)h; (void)nlimbs; (void)exp_bits; (void)count; (void)cfg;
-  return false;
+
+static const int kTpi[6] = {1, 2, 4, 8, 16, 32};
+static const int kThreads[4] = {32, 64, 128, 256};
+
+bool powm_candidate(uint32_t nlimbs, int slot, PowmConfig *cfg) {
+  if (slot < 0 || slot >= kPowmDists * kPowmWindows || nlimbs == 0) return false;
+  int d = slot / kPowmWindows;
+  PowmConfig c;
+  c.window = slot % kPowmWindows + 1;
+  if (d == kPowmDists - 1) {
+    c.dist = kDistDigit;
+    *cfg = c;
+    return true;
+  }
+  c.dist = kDistLanes;
+  c.tpi = kTpi[d];
+  int best = 0;
+  for (const auto &e : powm_registry())
+    if (e.tpi == c.tpi && (uint32_t)e.tpi * e.limbs >= nlimbs && (best == 0 || e.limbs < best)) best = e.limbs;
+  if (!best) return false;
+  c.limbs = best;
+  *cfg = c;
+  return true;
 }
-void tuner_destroy(xmpHandle_t h) { (void)h; }
+
+int elem_threads(int slot) { return kThreads[slot % 4]; }
+
+bool elem_candidate(int op, uint32_t nlimbs, int slot, ElemConfig *cfg) {
+  if (slot < 0 || slot >= kElemSlots || nlimbs == 0) return false;
+  ElemConfig c;
+  c.variant = slot / 4;
+  c.threads = kThreads[slot % 4];
+  if (c.variant == 0) {
+    bool ok = (op == xmpTuneMul) ? mul_has_register_kernel(nlimbs, nlimbs) : div_has_register_kernel(nlimbs);
+    if (!ok) return false;
+  }
+  *cfg = c;
+  return true;
+}
+
+TunerState *tuner_state(xmpHandle_t h) {
+  if (!h->tuner) h->tuner = new TunerState();
+  return reinterpret_cast<TunerState *>(h->tuner);
+}
+
+void tuner_destroy(xmpHandle_t h) {
+  if (h->tuner) delete reinterpret_cast<TunerState *>(h->tuner);
+  h->tuner = nullptr;
+}
+
+// op (2 bits) | limbs (14 bits) | exponent bits (16 bits) | count (32 bits)
+uint64_t shape_key(int op, uint32_t bits, uint32_t exp_bits, uint32_t count) {
+  return ((uint64_t)(op & 3) << 62) | ((uint64_t)((bits / 32) & 0x3fff) << 48) |
+         ((uint64_t)(exp_bits & 0xffff) << 32) | (uint64_t)count;
+}
+
+int count_bucket(uint32_t count) {
+  int b = 31 - __builtin_clz(count ? count : 1);
+  return std::min(b, kGridCountBuckets - 1);
+}
+
+int exp_bucket(uint32_t exp_bits) {
+  int b = 31 - __builtin_clz(exp_bits ? exp_bits : 1);
+  return std::min(b, kGridExpBuckets - 1);
+}
+
+size_t grid_index(int op, uint32_t nlimbs, int cb, int eb) {
+  return (((size_t)op * kGridMaxLimbs + (nlimbs - 1)) * kGridCountBuckets + cb) * kGridExpBuckets + eb;
+}
+
+int tuner_lookup(xmpHandle_t h, int op, uint32_t bits, uint32_t exp_bits, uint32_t count, int *source) {
+  if (source) *source = 0;
+  if (!h->tuner) return -1;
+  TunerState *t = reinterpret_cast<TunerState *>(h->tuner);
+  auto it = t->choices.find(shape_key(op, bits, op == xmpTunePowm ? exp_bits : 0, count));
+  if (it != t->choices.end()) {
+    if (source) *source = 1;
+    return it->second;
+  }
+  uint32_t nl = bits / 32;
+  if (t->has_table && nl >= 1 && nl <= (uint32_t)kGridMaxLimbs) {
+    int slot = t->table[grid_index(op, nl, count_bucket(count), op == xmpTunePowm ? exp_bucket(exp_bits) : 0)];
+    if (slot != 0xff) {
+      if (source) *source = 2;
+      return slot;
+    }
+  }
+  return -1;
+}
+
+bool tuner_lookup_powm(xmpHandle_t h, uint32_t nlimbs, uint32_t exp_bits, uint32_t count, PowmConfig *cfg) {
+  int slot = tuner_lookup(h, xmpTunePowm, nlimbs * 32, exp_bits, count, nullptr);
+  return slot >= 0 && powm_candidate(nlimbs, slot, cfg);
+}
+
+// ---- synthetic data for the exhaustive tuner ----------------------------------
+// mode 0: uniform limbs; 1: odd modulus with the top bit set; 2: exactly `bits` bits (top bit set)
+__global__ void fill_kernel(uint32_t *limbs, uint32_t nlimbs, uint32_t stride, uint32_t count, uint64_t seed,
+                            int mode, uint32_t bits) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  uint64_t s = seed ^ (0x9E3779B97F4A7C15ull * (i + 1));
+  for (uint32_t j = 0; j < round_up(nlimbs, 4); j++) {
+    s += 0x9E3779B97F4A7C15ull;
+    uint64_t z = s;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    uint32_t v = (uint32_t)z;
+    if (j >= nlimbs) v = 0;
+    if (mode == 1 && j == 0) v |= 1u;
+    if (mode == 1 && j == nlimbs - 1) v |= 0x80000000u;
+    if (mode == 2) {
+      uint32_t lo = j * 32;
+      if (lo >= bits) v = 0;
+      else if (bits - lo <= 32) {
+        uint32_t nb = bits - lo;
+        v = (nb == 32 ? v : (v & ((1u << nb) - 1u))) | (1u << (nb - 1));
+      }
+    }
+    limbs[((size_t)(j >> 2) * stride + i) * 4 + (j & 3)] = v;
+  }
+}
+
+static void fill(xmpHandle_t h, xmpIntegers_t x, uint64_t seed, int mode, uint32_t bits) {
+  fill_kernel<<<grid_for(x->count, 128), 128, 0, h->stream>>>(x->limbs, x->nlimbs, x->stride, x->count, seed, mode,
+                                                               bits);
+}
+
 }  // namespace xmpb
+
+extern "C" {
+
+xmpError_t XMPAPI xmpTuneCandidate(int32_t op, uint32_t bits, int32_t slot, int32_t *valid, xmpPowmConfig_t *config) {
+  if (!valid || bits == 0 || bits % 32) return xmpErrorInvalidParameter;
+  *valid = 0;
+  if (op == xmpTunePowm) {
+    PowmConfig c;
+    if (powm_candidate(bits / 32, slot, &c)) {
+      *valid = 1;
+      if (config) *config = xmpPowmConfig_t{c.dist, c.tpi, c.limbs, c.window};
+    }
+  } else if (op == xmpTuneMul || op == xmpTuneDivMod) {
+    ElemConfig c;
+    if (elem_candidate(op, bits / 32, slot, &c)) {
+      *valid = 1;
+      if (config) *config = xmpPowmConfig_t{c.variant, c.threads, 0, 0};
+    }
+  } else {
+    return xmpErrorInvalidParameter;
+  }
+  return xmpErrorSuccess;
+}
+
+xmpError_t XMPAPI xmpTuneMeasure(xmpHandle_t h, const xmpTuneShape_t *shape, int32_t reps, float *ms) {
+  if (!h || !shape || !ms || shape->bits == 0 || shape->bits % 32 || shape->count == 0) return xmpErrorInvalidParameter;
+  if (shape->op == xmpTunePowm && (shape->exp_bits == 0)) return xmpErrorInvalidParameter;
+  DeviceGuard guard(h->device);
+  const uint32_t bits = shape->bits, count = shape->count;
+  for (int s = 0; s < kCand; s++) ms[s] = -1.0f;
+  xmpIntegers_t a = nullptr, b = nullptr, c = nullptr, d = nullptr;
+  xmpError_t e = xmpErrorSuccess;
+  auto cleanup = [&]() {
+    cudaStreamSynchronize(h->stream);
+    for (xmpIntegers_t x : {a, b, c, d})
+      if (x) xmpIntegersDestroy(h, x);
+  };
+  const uint64_t seed = 0x5EEDull * bits + count;
+  if (shape->op == xmpTunePowm) {
+    uint32_t eprec = round_up(shape->exp_bits, 32);
+    if ((e = xmpIntegersCreate(h, &a, bits, count)) || (e = xmpIntegersCreate(h, &b, eprec, count)) ||
+        (e = xmpIntegersCreate(h, &c, bits, count)) || (e = xmpIntegersCreate(h, &d, bits, count))) {
+      cleanup();
+      return e;
+    }
+    fill(h, a, seed, 0, bits);
+    fill(h, b, seed + 1, 2, shape->exp_bits);
+    fill(h, c, seed + 2, 1, bits);
+  } else {
+    uint32_t abits = shape->op == xmpTuneDivMod ? 2 * bits : bits;
+    if ((e = xmpIntegersCreate(h, &a, abits, count)) || (e = xmpIntegersCreate(h, &b, bits, count)) ||
+        (e = xmpIntegersCreate(h, &c, 2 * bits, count)) || (e = xmpIntegersCreate(h, &d, bits, count))) {
+      cleanup();
+      return e;
+    }
+    fill(h, a, seed, 0, abits);
+    fill(h, b, seed + 1, 1, bits);
+  }
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  // Policy without index arrays for the timed runs.
+  xmpExecutionPolicy_t saved = h->policy;
+  h->policy = &h->default_policy;
+  float best = 1e30f;
+  bool hopeless[kPowmDists] = {false};
+  for (int s = 0; s < kCand && e == xmpErrorSuccess; s++) {
+    PowmConfig pc;
+    ElemConfig ec;
+    bool ok = shape->op == xmpTunePowm ? powm_candidate(bits / 32, s, &pc) : elem_candidate(shape->op, bits / 32, s, &ec);
+    if (!ok) continue;
+    const int dist = shape->op == xmpTunePowm ? s / kPowmWindows : s / 4;
+    if (hopeless[dist]) {
+      ms[s] = NAN;  // valid, not timed: this distribution was already far slower than the best
+      continue;
+    }
+    auto run = [&]() -> xmpError_t {
+      if (shape->op == xmpTunePowm) {
+        xmpPowmConfig_t cfg{pc.dist, pc.tpi, pc.limbs, pc.window};
+        return xmpIntegersPowmWithConfigAsync(h, d, a, b, c, count, &cfg);
+      }
+      if (shape->op == xmpTuneMul) return mul_entry(h, c, a, b, count, &ec);
+      return divmod_entry(h, c, d, a, b, count, &ec);
+    };
+    float t = 1e30f;
+    int runs = std::max(1, (int)reps);
+    for (int r = 0; r < runs + 1 && e == xmpErrorSuccess; r++) {
+      cudaEventRecord(t0, h->stream);
+      e = run();
+      cudaEventRecord(t1, h->stream);
+      cudaEventSynchronize(t1);
+      float f = 0;
+      cudaEventElapsedTime(&f, t0, t1);
+      if (r > 0 || runs == 1) t = std::min(t, f);
+      // A candidate far slower than the best so far is not repeated, and the
+      // other windows of its distribution are not timed at all.
+      if (r == 0 && f > 10.0f * best && f > 20.0f) {
+        t = f;
+        if (f > 20.0f * best) hopeless[dist] = true;
+        break;
+      }
+    }
+    if (e != xmpErrorSuccess) break;
+    ms[s] = t;
+    best = std::min(best, t);
+  }
+  h->policy = saved;
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  cleanup();
+  if (e != xmpErrorSuccess) return e;
+  return check_cuda();
+}
+
+xmpError_t XMPAPI xmpTuneSetChoice(xmpHandle_t h, const xmpTuneShape_t *shape, int32_t slot) {
+  if (!h || !shape || slot < 0 || slot >= kCand) return xmpErrorInvalidParameter;
+  tuner_state(h)->choices[shape_key(shape->op, shape->bits, shape->op == xmpTunePowm ? shape->exp_bits : 0,
+                                    shape->count)] = slot;
+  return xmpErrorSuccess;
+}
+
+xmpError_t XMPAPI xmpTuneGetChoice(xmpHandle_t h, const xmpTuneShape_t *shape, int32_t *slot, int32_t *source) {
+  if (!h || !shape || !slot) return xmpErrorInvalidParameter;
+  int src = 0;
+  int s = tuner_lookup(h, shape->op, shape->bits, shape->exp_bits, shape->count, &src);
+  if (s < 0) {
+    // the heuristic's choice expressed as a slot
+    if (shape->op == xmpTunePowm) {
+      PowmConfig c = powm_default_config(shape->bits / 32, shape->exp_bits, shape->count, xmpAlgorithmDefault,
+                                         h->sm_count);
+      int d = c.dist == kDistDigit ? kPowmDists - 1 : 0;
+      if (c.dist != kDistDigit)
+        for (int k = 0; k < 6; k++)
+          if (kTpi[k] == c.tpi) d = k;
+      s = d * kPowmWindows + std::min(c.window, kPowmWindows) - 1;
+    } else {
+      bool reg = shape->op == xmpTuneMul ? mul_has_register_kernel(shape->bits / 32, shape->bits / 32)
+                                         : div_has_register_kernel(shape->bits / 32);
+      s = (reg ? 0 : 4) + 2;  // 128 threads
+    }
+    src = 0;
+  }
+  *slot = s;
+  if (source) *source = src;
+  return xmpErrorSuccess;
+}
+
+xmpError_t XMPAPI xmpTuneClear(xmpHandle_t h) {
+  if (!h) return xmpErrorInvalidParameter;
+  TunerState *t = tuner_state(h);
+  t->choices.clear();
+  t->table.clear();
+  t->has_table = false;
+  return xmpErrorSuccess;
+}
+
+xmpError_t XMPAPI xmpSelectorLoad(xmpHandle_t h, const float *params) {
+  if (!h || !params) return xmpErrorInvalidParameter;
+  DeviceGuard guard(h->device);
+  TunerState *t = tuner_state(h);
+  xmpError_t e = selector_fill_table(h, params, &t->table);
+  t->has_table = (e == xmpErrorSuccess);
+  return e;
+}
+
+}  // extern "C"
