@@ -306,6 +306,136 @@ def run_ours(args, rank, world, local_rank):
     h.destroy()
 
 
+def _crt_keys(nkeys, half_bits, seed):
+    """RSA keys from GMP nextprime on seeded random starts (oracle generators, CPU)."""
+    import oracle as orc
+    keys, s = [], seed
+    while len(keys) < nkeys:
+        p0 = orc.random_limbs(s, 1, half_bits // 32)[0]
+        q0 = orc.random_limbs(s + 1, 1, half_bits // 32)[0]
+        p0[-1] |= np.uint32(0x80000000)
+        q0[-1] |= np.uint32(0x80000000)
+        s += 2
+        k = orc.crt_key(p0, q0)
+        if k is not None and orc.to_int(k["p"]) != orc.to_int(k["q"]):
+            keys.append(k)
+    return keys
+
+
+def run_mixed(args):
+    """Uneven-size batch: 65,536 instances (40% 1024, 30% 2048, 20% 3072, 10% 4096 bits,
+    full-length exponents, bases in [0, m)) plus 16,384 CRT-RSA private operations
+    (1024-bit primes from nextprime, e = 65537, Garner with q^-1 mod p, messages
+    uniform in [0, pq)).  Plain per-size xmpIntegersPowm calls and the CRT op
+    sequence vs one autotuned batch plan replayed as a CUDA graph."""
+    import torch
+    import oracle as orc
+    import xmp_b200 as xmp
+    from xmp_b200 import tuning
+    torch.cuda.set_device(0)
+    total, ncrt, nkeys = args.count, args.crt, args.crt_keys
+    mix = [(1024, 0.4), (2048, 0.3), (3072, 0.2), (4096, 0.1)]
+    sizes = [(b, int(total * f)) for b, f in mix]
+    sizes[0] = (1024, total - sum(c for _, c in sizes[1:]))
+    keys = _crt_keys(nkeys, 1024, 777)
+    rng = np.random.default_rng(778)
+    h = xmp.Handle()
+    stream = torch.cuda.current_stream()
+    h.set_stream(stream.cuda_stream)
+    groups = []
+    for k, (bits, cnt) in enumerate(sizes):
+        n = bits // 32
+        m = orc.full_length_odd(900 + k, cnt, n)
+        x = orc.below(910 + k, m)
+        e = orc.random_limbs(920 + k, cnt, n)
+        e[:, -1] |= np.uint32(0x80000000)
+        X, E, M = (h.integers(bits, cnt, v) for v in (x, e, m))
+        groups.append(dict(bits=bits, count=cnt, X=X, E=E, M=M, O1=h.integers(bits, cnt), O2=h.integers(bits, cnt),
+                           sample=(x[:16], e[:16], m[:16])))
+    msgs, cts = [], []
+    for i in range(ncrt):
+        kk = keys[i % nkeys]
+        nn = orc.to_int(kk["n"])
+        mm = int.from_bytes(rng.bytes(256), "little") % nn
+        msgs.append(mm)
+        cts.append(pow(mm, 65537, nn))
+    C = h.integers(2048, ncrt, np.stack([orc.from_int(c, 64) for c in cts]))
+    ka = {f: h.integers(1024, nkeys, np.stack([kk[f] for kk in keys])) for f in ("p", "q", "dp", "dq", "qinv")}
+    outs = [h.integers(2048, ncrt) for _ in range(2)]
+    tmp = dict(cp=h.integers(1024, ncrt), cq=h.integers(1024, ncrt), mp=h.integers(1024, ncrt),
+               mq=h.integers(1024, ncrt), p2=h.integers(1056, nkeys), t1=h.integers(1056, ncrt),
+               d=h.integers(1056, ncrt), e=h.integers(2080, ncrt), hh=h.integers(1024, ncrt), f=h.integers(2048, ncrt))
+
+    def plain():
+        for g in groups:
+            xmp.check(xmp.lib().xmpIntegersPowmAsync(h.h, g["O1"].x, g["X"].x, g["E"].x, g["M"].x, g["count"]))
+        L = xmp.lib()
+        xmp.check(L.xmpIntegersModAsync(h.h, tmp["cp"].x, C.x, ka["p"].x, ncrt))
+        xmp.check(L.xmpIntegersModAsync(h.h, tmp["cq"].x, C.x, ka["q"].x, ncrt))
+        xmp.check(L.xmpIntegersPowmAsync(h.h, tmp["mp"].x, tmp["cp"].x, ka["dp"].x, ka["p"].x, ncrt))
+        xmp.check(L.xmpIntegersPowmAsync(h.h, tmp["mq"].x, tmp["cq"].x, ka["dq"].x, ka["q"].x, ncrt))
+        xmp.check(L.xmpIntegersAddAsync(h.h, tmp["p2"].x, ka["p"].x, ka["p"].x, nkeys))
+        xmp.check(L.xmpIntegersAddAsync(h.h, tmp["t1"].x, tmp["mp"].x, tmp["p2"].x, ncrt))
+        xmp.check(L.xmpIntegersSubAsync(h.h, tmp["d"].x, tmp["t1"].x, tmp["mq"].x, ncrt))
+        xmp.check(L.xmpIntegersMulAsync(h.h, tmp["e"].x, tmp["d"].x, ka["qinv"].x, ncrt))
+        xmp.check(L.xmpIntegersModAsync(h.h, tmp["hh"].x, tmp["e"].x, ka["p"].x, ncrt))
+        xmp.check(L.xmpIntegersMulAsync(h.h, tmp["f"].x, ka["q"].x, tmp["hh"].x, ncrt))
+        xmp.check(L.xmpIntegersAddAsync(h.h, outs[0].x, tmp["f"].x, tmp["mq"].x, ncrt))
+
+    # autotuned batch plan (learned selector installed when its weights exist), replayed as a graph
+    selector = os.path.exists(tuning.DEFAULT_WEIGHTS)
+    if selector:
+        tuning.install(h, tuning.load_weights())
+    plan = xmp.BatchPlan(h, [(g["O2"], g["X"], g["E"], g["M"], g["count"]) for g in groups],
+                         [(outs[1], C, ka["p"], ka["q"], ka["dp"], ka["dq"], ka["qinv"], ncrt)], use_graph=True)
+
+    def timed(fn, steps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return float(np.median(ts))
+
+    # plain launches run with the built-in heuristic only (no tuned entries)
+    xmp.check(xmp.lib().xmpTuneClear(h.h))
+    t_plain = timed(plain, args.steps, args.warmup)
+    t_batch = timed(plan.execute, args.steps, args.warmup)
+    # the plain launches one at a time: their sum bounds what any schedule of the same kernels can gain
+    parts = {}
+    for g in groups:
+        parts["powm%d" % g["bits"]] = timed(lambda g=g: xmp.check(xmp.lib().xmpIntegersPowmAsync(
+            h.h, g["O1"].x, g["X"].x, g["E"].x, g["M"].x, g["count"])), 2, 1)
+    parts["crt"] = t_plain - sum(parts.values())
+    ok = all(np.array_equal(g["O1"].export(), g["O2"].export()) for g in groups)
+    res = [orc.to_int(r) for r in outs[1].export()[:256]]
+    ok = ok and res == msgs[:256] and np.array_equal(outs[0].export(), outs[1].export())
+    x, e, m = groups[1]["sample"]
+    want, _ = orc.powm(x, e, m, len(m))
+    ok = ok and np.array_equal(groups[1]["O2"].export()[:16], want)
+    n_ops = total + ncrt
+    line = {"metric": "mixed-size batch speedup (autotuned batch plan vs plain per-size launches)",
+            "value": t_plain / t_batch, "unit": "x", "higher_is_better": True, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_batch, "dtype": "u32", "data": "synthetic (seeded)",
+            "config": {"workload": "65,536 mixed powm (40/30/20/10%% of 1024/2048/3072/4096 bits) + %d CRT-RSA-2048"
+                       % ncrt, "crt_keys": nkeys, "selector": selector},
+            "plain_ms": t_plain, "batch_ms": t_batch, "plain_parts_ms": parts, "plain_ops_per_s": n_ops / (t_plain * 1e-3),
+            "batch_ops_per_s": n_ops / (t_batch * 1e-3),
+            "bins": [dict(precision=b["precision"], count=b["count"], blocks=b["blocks"],
+                          lanes=b["config"].lanes, limbs=b["config"].limbs, window=b["config"].window)
+                     for b in plan.info()],
+            "result_check": ok}
+    print(json.dumps(line), flush=True)
+    plan.destroy()
+    h.destroy()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -318,7 +448,13 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--workload", default="powm2048", choices=["powm2048", "mixed"])
+    ap.add_argument("--crt", type=int, default=16384)
+    ap.add_argument("--crt-keys", type=int, default=256)
     args = ap.parse_args()
+    if args.workload == "mixed":
+        run_mixed(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

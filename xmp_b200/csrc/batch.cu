@@ -128,28 +128,32 @@ static xmpError_t enqueue(xmpHandle_t h, xmpPowmBatchPlan_t p, cudaStream_t main
       if ((r = xmpIntegersModAsync(h, p->temps[c].cq, it.c, it.q, it.count))) return r;
     }
     if (cudaEventRecord(p->fork, main) != cudaSuccess) return xmpErrorCuda;
+    // every bin on its own stream, in launch order (longest instances first);
+    // the Garner recombination follows the bin holding the CRT halves
     int side = 0;
-    for (size_t b = 1; b < p->bins.size(); b++) {
+    for (size_t b = 0; b < p->bins.size(); b++) {
       if (p->bins[b].serial) continue;
       cudaStream_t s = p->side[side];
       if (cudaStreamWaitEvent(s, p->fork, 0) != cudaSuccess) return xmpErrorCuda;
       if ((r = launch_bin(h, p, (int)b, s))) return r;
+      if (p->bins[b].has_crt) {
+        h->stream = s;
+        for (size_t c = 0; c < p->crt.size(); c++) {
+          const xmpPowmCRTItem_t &it = p->crt[c];
+          const CrtTemps &t = p->temps[c];
+          const uint32_t n = it.count;
+          if ((r = xmpIntegersAddAsync(h, t.p2, it.p, it.p, n))) return r;    // 2p
+          if ((r = xmpIntegersAddAsync(h, t.t1, t.mp, t.p2, n))) return r;    // mp + 2p
+          if ((r = xmpIntegersSubAsync(h, t.d, t.t1, t.mq, n))) return r;     // mp + 2p - mq in (0, 3p)
+          if ((r = xmpIntegersMulAsync(h, t.e, t.d, it.qinv, n))) return r;   // d * qinv
+          if ((r = xmpIntegersModAsync(h, t.hh, t.e, it.p, n))) return r;     // h = d * qinv mod p
+          if ((r = xmpIntegersMulAsync(h, t.f, it.q, t.hh, n))) return r;     // q * h
+          if ((r = xmpIntegersAddAsync(h, it.out, t.f, t.mq, n))) return r;   // mq + q * h
+        }
+        h->stream = main;
+      }
       if (cudaEventRecord(p->joins[side], s) != cudaSuccess) return xmpErrorCuda;
       side++;
-    }
-    if (!p->bins.empty() && !p->bins[0].serial && (r = launch_bin(h, p, 0, main))) return r;
-    // Garner recombination right after the bin holding the CRT halves (bin 0).
-    for (size_t c = 0; c < p->crt.size(); c++) {
-      const xmpPowmCRTItem_t &it = p->crt[c];
-      const CrtTemps &t = p->temps[c];
-      const uint32_t n = it.count;
-      if ((r = xmpIntegersAddAsync(h, t.p2, it.p, it.p, n))) return r;    // 2p
-      if ((r = xmpIntegersAddAsync(h, t.t1, t.mp, t.p2, n))) return r;    // mp + 2p
-      if ((r = xmpIntegersSubAsync(h, t.d, t.t1, t.mq, n))) return r;     // mp + 2p - mq in (0, 3p)
-      if ((r = xmpIntegersMulAsync(h, t.e, t.d, it.qinv, n))) return r;   // d * qinv
-      if ((r = xmpIntegersModAsync(h, t.hh, t.e, it.p, n))) return r;     // h = d * qinv mod p
-      if ((r = xmpIntegersMulAsync(h, t.f, it.q, t.hh, n))) return r;     // q * h
-      if ((r = xmpIntegersAddAsync(h, it.out, t.f, t.mq, n))) return r;   // mq + q * h
     }
     for (int j = 0; j < side; j++)
       if (cudaStreamWaitEvent(main, p->joins[j], 0) != cudaSuccess) return xmpErrorCuda;
@@ -167,13 +171,6 @@ static xmpError_t enqueue(xmpHandle_t h, xmpPowmBatchPlan_t p, cudaStream_t main
   h->stream = saved_stream;
   h->policy = saved_policy;
   return e;
-}
-
-static uint64_t bin_work(const BatchBin &b) {
-  uint64_t cap = b.cfg.dist == kDistDigit ? b.nlimbs : (uint64_t)b.cfg.tpi * b.cfg.limbs;
-  uint64_t w = 0;
-  for (const BatchSegment &s : b.segs) w += (uint64_t)s.count * cap * cap * std::max<uint32_t>(s.exp->precision, 32);
-  return w;
 }
 
 }  // namespace xmpb
@@ -252,20 +249,27 @@ xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t h, const xmpPowmBatchItem_t
       bin->has_crt |= seg_is_crt[i];
     }
   }
-  // bin 0 runs on the handle's stream: the CRT bin if any, else the largest
-  if (!p->bins.empty() && !p->bins[0].has_crt) {
-    size_t best = 0;
-    for (size_t b = 1; b < p->bins.size(); b++)
-      if (p->bins[b].count * (uint64_t)p->bins[b].nlimbs > p->bins[best].count * (uint64_t)p->bins[best].nlimbs)
-        best = b;
-    std::swap(p->bins[0], p->bins[best]);
-  }
-  // ---- configurations and CTA shares ----
-  uint64_t total_work = 0;
+  // ---- configurations and grids ----
+  // Every bin gets a full persistent grid (SMs x resident CTAs) and all bins
+  // are launched at once, longest instances first: the block scheduler runs
+  // them back to back at full width and fills each bin's tail with the next
+  // bin's CTAs, with no work estimate to get wrong.  Lanes and limbs are the
+  // tuner's choice at a saturating batch (an exact tuned entry for the bin's
+  // own shape wins); the window follows the exponent length.
+  const uint32_t kSaturated = 1u << 16;
   for (auto &b : p->bins) {
     PowmConfig c;
-    bool tuned = tuner_lookup_powm(h, b.nlimbs, b.exp_bits, b.count, &c) && c.dist == kDistLanes;
-    if (!tuned) c = powm_default_config(b.nlimbs, b.exp_bits, b.count, xmpAlgorithmDefault, h->sm_count);
+    int src = 0;
+    bool exact = tuner_lookup(h, xmpTunePowm, b.nlimbs * 32, b.exp_bits, b.count, &src) >= 0 && src == 1 &&
+                 tuner_lookup_powm(h, b.nlimbs, b.exp_bits, b.count, &c) && c.dist == kDistLanes;
+    if (!exact) {
+      bool tuned = tuner_lookup_powm(h, b.nlimbs, b.exp_bits, std::max(b.count, kSaturated), &c) &&
+                   c.dist == kDistLanes;
+      if (!tuned)
+        c = powm_default_config(b.nlimbs, b.exp_bits, std::max(b.count, kSaturated), xmpAlgorithmDefault,
+                                h->sm_count);
+      c.window = window_for_bits(b.exp_bits);
+    }
     if (c.dist == kDistDigit) {
       // prefer any register kernel that holds the precision; else digit-serial after the join
       PowmConfig r = powm_default_config(b.nlimbs, b.exp_bits, b.count, xmpAlgorithmDistributedMP, h->sm_count);
@@ -277,8 +281,11 @@ xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t h, const xmpPowmBatchItem_t
       b.k = powm_find(c.tpi, c.limbs);
       if (!b.k) return fail(xmpErrorUnsupported);
     }
-    total_work += bin_work(b);
   }
+  // launch order: longest instances (work per instance) first
+  std::stable_sort(p->bins.begin(), p->bins.end(), [](const BatchBin &x, const BatchBin &y) {
+    return (uint64_t)x.nlimbs * x.nlimbs * x.exp_bits > (uint64_t)y.nlimbs * y.nlimbs * y.exp_bits;
+  });
   size_t bytes = 0;
   for (auto &b : p->bins) {
     if (b.serial) continue;
@@ -288,8 +295,7 @@ xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t h, const xmpPowmBatchItem_t
     const uint32_t per_item = 32 / b.cfg.tpi;
     uint64_t items = 0;
     for (const BatchSegment &s : b.segs) items += div_up(s.count, per_item);
-    double share = total_work ? (double)bin_work(b) / (double)total_work : 1.0;
-    uint64_t blocks = (uint64_t)std::llround(share * h->sm_count * occ);
+    uint64_t blocks = (uint64_t)h->sm_count * occ;
     blocks = std::max<uint64_t>(1, std::min<uint64_t>(blocks, div_up((uint32_t)std::min<uint64_t>(items, 0xffffffffu), 4)));
     b.blocks = (int)blocks;
     // shrink the window if the tables would exceed the scratch limit
@@ -297,7 +303,7 @@ xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t h, const xmpPowmBatchItem_t
            (size_t)b.blocks * 128 * b.cfg.limbs * ((size_t)4 << b.cfg.window) > scratch_limit(h) / 2)
       b.cfg.window--;
     b.table_offset = bytes;
-    bytes += round_up((uint32_t)0, 1) + (size_t)b.blocks * 128 * b.cfg.limbs * ((size_t)4 << b.cfg.window);
+    bytes += (size_t)b.blocks * 128 * b.cfg.limbs * ((size_t)4 << b.cfg.window);
     bytes = (bytes + 255) & ~(size_t)255;
   }
   size_t counter_offset = bytes;
@@ -309,7 +315,7 @@ xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t h, const xmpPowmBatchItem_t
   if (p->bins.size() > 64) return fail(xmpErrorUnsupported);
   // ---- streams and events ----
   if (cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) != cudaSuccess) return fail(xmpErrorCuda);
-  for (size_t b = 1; b < p->bins.size(); b++) {
+  for (size_t b = 0; b < p->bins.size(); b++) {
     if (p->bins[b].serial) continue;
     cudaStream_t s;
     cudaEvent_t ev;

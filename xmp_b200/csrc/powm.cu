@@ -48,7 +48,7 @@ bool powm_config_valid(const PowmConfig &c, uint32_t nlimbs) {
 }
 
 PowmConfig powm_default_config(uint32_t nlimbs, uint32_t exp_bits, uint32_t count, xmpAlgorithm_t alg,
-                               uint32_t sm_count) {
+                               uint32_t sm_count, uint32_t want_cap) {
   PowmConfig best;
   best.window = window_for_bits(exp_bits);
   if (alg == xmpAlgorithmDigitMP) {
@@ -62,7 +62,7 @@ PowmConfig powm_default_config(uint32_t nlimbs, uint32_t exp_bits, uint32_t coun
     if (alg == xmpAlgorithmRegMP && e.tpi != 1) continue;
     if (alg == xmpAlgorithmDistributedMP && e.tpi == 1) continue;
     uint32_t cap = (uint32_t)e.tpi * e.limbs;
-    if (cap < nlimbs) continue;
+    if (cap < nlimbs || (want_cap && cap != want_cap)) continue;
     // Work per instance grows with capacity^2; lane overhead (shfl, carry
     // bookkeeping) is ~12 instructions per 4L multiply-adds.
     double pad = (double)cap / nlimbs;

@@ -60,8 +60,10 @@ struct PowmKernelRegistrar {
 int window_for_bits(uint32_t exp_bits);
 
 // Heuristic configuration for n-limb moduli (used when no tuned entry exists).
+// A nonzero `cap` admits only kernels with exactly cap = lanes x limbs (the
+// Montgomery radix R = 2^(32 cap) of precomputed constants).
 PowmConfig powm_default_config(uint32_t nlimbs, uint32_t exp_bits, uint32_t count, xmpAlgorithm_t alg,
-                               uint32_t sm_count);
+                               uint32_t sm_count, uint32_t cap = 0);
 bool powm_config_valid(const PowmConfig &c, uint32_t nlimbs);
 
 // Runs out = base^exp mod mod for `count` op instances starting at 0 with the

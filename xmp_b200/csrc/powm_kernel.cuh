@@ -225,15 +225,16 @@ __global__ void __launch_bounds__(128) powm_kernel(PowmArgs args) {
   powm_instance<TPI, L>(G, args, i, valid, slot);
 }
 
-// R^2 mod N (R = 2^(32 * TPI * L)) for every element of `args.mod`, written
-// to `args.out` (server set-up: Montgomery constants kept on the device).
+// R^2 mod N (R = 2^(32 * TPI * L)) for elements start .. start+count-1 of
+// `args.mod`, written to the same elements of `args.out` (serving set-up:
+// Montgomery constants kept on the device).
 template <int TPI, int L>
 __global__ void __launch_bounds__(128) r2_kernel(PowmArgs args) {
   Group<TPI> G;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t local = gtid / TPI;
   const bool valid = local < args.count;
-  const uint32_t i = valid ? local : args.count - 1;
+  const uint32_t i = args.start + (valid ? local : args.count - 1);
   uint32_t n[L], r2[L];
   load_lane_limbs<TPI, L>(n, args.mod.limbs, args.mod.nlimbs, args.mod.stride, i, G.lane);
   const uint32_t np0 = neg_inv32(G.bcast(n[0], 0));
