@@ -436,6 +436,233 @@ def run_mixed(args):
     h.destroy()
 
 
+def run_serve(args):
+    """Serving loop: open-loop Poisson arrivals of requests with 1-64 ops under
+    one key from a pool of 1,024 odd full-length moduli (512 x 2048, 307 x
+    3072, 205 x 4096 bits: a 50/30/20 mix), bases below the key, full-length
+    exponents; 8 GiB HBM admission budget.  Peak = saturated throughput (all
+    requests at t=0); the sweep reports p50/p99/p999 per offered rate; the
+    baseline is plain synchronous per-request calls."""
+    # one hardware queue per server stream (read when the CUDA context is created)
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+    import torch
+    import oracle as orc
+    import xmp_b200 as xmp
+    from xmp_b200 import tuning
+    torch.cuda.set_device(0)
+    h = xmp.Handle()
+    selector = os.path.exists(tuning.DEFAULT_WEIGHTS)
+    if selector:
+        tuning.install(h, tuning.load_weights())
+    classes = [(2048, 512), (3072, 307), (4096, 205)]
+    srv = xmp.Server(h, [c for c, _ in classes], hbm_budget=8 << 30, max_keys=512)
+    # per class: one block of 64 ops per key (bases below that key); a request
+    # takes the first nops ops of a block, results land in that block's rows
+    blocks = []
+    for ci, (bits, nk) in enumerate(classes):
+        n = bits // 32
+        keys = orc.full_length_odd(5000 + ci, nk, n)
+        first = srv.add_keys(bits, keys)
+        mm = np.repeat(keys, 64, axis=0)
+        base = orc.below(5100 + ci, mm).reshape(nk, 64, n)
+        exp = orc.random_limbs(5200 + ci, nk * 64, n)
+        exp[:, -1] |= np.uint32(0x80000000)
+        exp = exp.reshape(nk, 64, n)
+        out = np.zeros_like(base)
+        for k in range(nk):
+            blocks.append((first + k, base[k], exp[k], out[k], keys[k], bits))
+    rng = np.random.default_rng(4242)
+
+    def stream(n_req, rate):
+        """n_req requests; arrival times (ns) of a Poisson process at `rate` ops/s (0: all at once)."""
+        ks = rng.integers(0, len(blocks), size=n_req)
+        nops = rng.integers(1, 65, size=n_req)
+        if rate > 0:
+            gaps = rng.exponential(32.5 / rate * 1e9, size=n_req)
+            arr = np.cumsum(gaps).astype(np.uint64)
+        else:
+            arr = np.zeros(n_req, dtype=np.uint64)
+        keys = [blocks[k][0] for k in ks]
+        bases = [blocks[k][1][:m] for k, m in zip(ks, nops)]
+        exps = [blocks[k][2][:m] for k, m in zip(ks, nops)]
+        outs = [blocks[k][3][:m] for k, m in zip(ks, nops)]
+        return keys, arr, bases, exps, outs, int(nops.sum()), ks, nops
+
+    def run(n_req, rate, mode=0):
+        keys, arr, bases, exps, outs, ops, ks, nops = stream(n_req, rate)
+        lat, secs = srv.replay(keys, arr, bases, exps, outs, mode=mode)
+        ms = lat.astype(np.float64) * 1e-6
+        return {"offered_ops_per_s": rate, "requests": n_req, "ops": ops, "ops_per_s": ops / secs,
+                "p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
+                "p999_ms": float(np.percentile(ms, 99.9)), "max_ms": float(ms.max())}, ks, nops
+
+    # latency floor: one op alone per size (median of 3)
+    floor = {}
+    for bits in (2048, 3072, 4096):
+        k = next(i for i, b in enumerate(blocks) if b[5] == bits)
+        t = []
+        for _ in range(3):
+            lat, _ = srv.replay([blocks[k][0]], np.zeros(1, np.uint64), [blocks[k][1][:1]], [blocks[k][2][:1]],
+                                [blocks[k][3][:1]])
+            t.append(float(lat[0]) * 1e-6)
+        floor[bits] = statistics.median(t)
+    run(200, 0)  # warm-up
+    peak, _, _ = run(args.serve_peak_requests, 0)
+    sweep = []
+    rates = sorted(set([10000, 25000, 50000, int(0.7 * peak["ops_per_s"]), 100000, 200000, 500000]))
+    at70 = None
+    for rate in rates:
+        n_req = max(50, int(rate * args.serve_seconds / 32.5))
+        r, _, _ = run(n_req, rate)
+        sweep.append(r)
+        if rate == int(0.7 * peak["ops_per_s"]):
+            at70 = r
+    sync, _, _ = run(args.serve_sync_requests, 10000, mode=1)
+    # results check: written rows of a sample of blocks against GMP
+    ok = True
+    for bi in rng.choice(len(blocks), size=12, replace=False):
+        key, base, exp, out, m, bits = blocks[bi]
+        rows = [j for j in range(8) if out[j].any()]  # rows some request wrote
+        if not rows:
+            continue
+        mm = np.repeat(m[None, :], len(rows), axis=0)
+        want, _ = orc.powm(base[rows], exp[rows], mm, len(rows))
+        ok = ok and np.array_equal(out[rows], want)
+    st = srv.stats()
+    line = {"metric": "serving p99 latency at 70% of peak load", "value": at70["p99_ms"], "unit": "ms",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "u32", "data": "synthetic (seeded)",
+            "config": {"workload": "open-loop Poisson modexp requests, 1-64 ops each, 1,024 keys "
+                                   "(50/30/20% of 2048/3072/4096 bits), full-length exponents",
+                       "hbm_budget_gib": 8, "selector": selector},
+            "peak_ops_per_s": peak["ops_per_s"], "at_70pct": at70, "sweep": sweep,
+            "sync_baseline": sync, "single_op_latency_ms": floor,
+            "server": {k: st[k] for k in ("waves", "admission_stalls", "max_inflight_ops", "device_bytes")},
+            "result_check": bool(ok)}
+    print(json.dumps(line), flush=True)
+    srv.destroy()
+    h.destroy()
+
+
+def run_elementwise(args):
+    """Elementwise and contraction suite: add, sub, and, ior, xor, not, shf (shifts
+    uniform 0..255), cmp, popc on 2^22 pairs of 256-bit operands (HBM-bound:
+    GB/s of algorithmic bytes against the measured HBM copy bandwidth); mul on
+    2^18 pairs of 512 x 512 -> 1024 bits; divmod on 2^18 instances of 2048-bit
+    dividends by 1024-bit divisors with the top bit set.  Operands resident in
+    HBM (every working set exceeds the 126 MB L2); each op checked bit-exact
+    against GMP on its first 4,096 instances; GMP multithreaded on the host
+    for add, mul and divmod."""
+    import torch
+    import oracle as orc
+    import xmp_b200 as xmp
+    torch.cuda.set_device(0)
+    h = xmp.Handle()
+    stream = torch.cuda.current_stream()
+    h.set_stream(stream.cuda_stream)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except (OSError, ValueError):
+        pass
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    imad_peak = probe_imad_peak()["imad"]
+    E = 1 << 22
+    a = orc.random_limbs(31, E, 8)
+    b = orc.random_limbs(32, E, 8)
+    sh = (orc.splitmix64(33, E) % np.uint64(256)).astype(np.int32)
+    A, B, C = h.integers(256, E, a), h.integers(256, E, b), h.integers(256, E)
+    SH = torch.from_numpy(sh).cuda()
+    I32 = torch.empty(E, dtype=torch.int32, device="cuda")
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    S = 4096
+    res = {}
+
+    def row(name, ms, bytes_per_op, count, ok, imad_per_op=0):
+        r = {"ms": ms, "ops_per_s": count / (ms * 1e-3), "bytes_per_op": bytes_per_op,
+             "gbs": bytes_per_op * count / (ms * 1e-3) / 1e9, "check": bool(ok)}
+        r["hbm_frac"] = r["gbs"] / hbm
+        if imad_per_op:
+            r["timad_s"] = imad_per_op * count / (ms * 1e-3) / 1e12
+            r["imad_frac"] = r["timad_s"] / imad_peak
+        res[name] = r
+
+    for name, fn, op in (("add", xmp.add, "add"), ("sub", xmp.sub, "sub"), ("and", xmp.and_, "and"),
+                         ("ior", xmp.ior, "ior"), ("xor", xmp.xor, "xor")):
+        ms = timed(lambda fn=fn: fn(h, C, A, B, E, asynchronous=True))
+        ok = np.array_equal(C.export(count=E)[:S], orc.binary(op, a[:S], b[:S], 8, S))
+        row(name, ms, 96, E, ok)
+    ms = timed(lambda: xmp.not_(h, C, A, E, asynchronous=True))
+    row("not", ms, 64, E, np.array_equal(C.export()[:S], orc.not_(a[:S], 8, S)))
+    L = xmp.lib()
+    ms = timed(lambda: xmp.check(L.xmpIntegersShfAsync(h.h, C.x, A.x, SH.data_ptr(), E, E)))
+    row("shf", ms, 68, E, np.array_equal(C.export()[:S], orc.shf(a[:S], sh[:S], 8, S)))
+    ms = timed(lambda: xmp.check(L.xmpIntegersCmpAsync(h.h, I32.data_ptr(), A.x, B.x, E)))
+    row("cmp", ms, 68, E, np.array_equal(I32[:S].cpu().numpy(), orc.cmp(a[:S], b[:S], S)))
+    ms = timed(lambda: xmp.check(L.xmpIntegersPopcAsync(h.h, I32.data_ptr(), A.x, E)))
+    row("popc", ms, 36, E, np.array_equal(I32[:S].cpu().numpy().view(np.uint32), orc.popc(a[:S], S)))
+    cpu = {}
+    t = time.perf_counter()
+    orc.binary("add", a, b, 8, E)
+    cpu["add"] = E / (time.perf_counter() - t)
+    for X in (A, B, C):
+        X.destroy()
+    # mul: 2^18 x (512 x 512 -> 1024)
+    M = 1 << 18
+    ma = orc.random_limbs(41, M, 16)
+    mb = orc.random_limbs(42, M, 16)
+    MA, MB, MC = h.integers(512, M, ma), h.integers(512, M, mb), h.integers(1024, M)
+    ms = timed(lambda: xmp.mul(h, MC, MA, MB, M, asynchronous=True))
+    row("mul", ms, 256, M, np.array_equal(MC.export()[:S], orc.binary("mul", ma[:S], mb[:S], 32, S)),
+        imad_per_op=2 * 16 * 16)
+    t = time.perf_counter()
+    orc.binary("mul", ma, mb, 32, M)
+    cpu["mul"] = M / (time.perf_counter() - t)
+    for X in (MA, MB, MC):
+        X.destroy()
+    # divmod: 2^18 x (2048 / 1024), divisor top bit set
+    da = orc.random_limbs(51, M, 64)
+    db = orc.random_limbs(52, M, 32)
+    db[:, -1] |= np.uint32(0x80000000)
+    DA, DB, DQ, DR = h.integers(2048, M, da), h.integers(1024, M, db), h.integers(2048, M), h.integers(1024, M)
+    ms = timed(lambda: xmp.divmod_(h, DQ, DR, DA, DB, M, asynchronous=True))
+    wq, wr = orc.divmod_(da[:S], db[:S], 64, 32, S)
+    row("divmod", ms, 256 + 128 + 256 + 128, M,
+        np.array_equal(DQ.export()[:S], wq) and np.array_equal(DR.export()[:S], wr),
+        imad_per_op=2 * (64 - 32 + 1) * 32)
+    t = time.perf_counter()
+    orc.divmod_(da, db, 64, 32, M)
+    cpu["divmod"] = M / (time.perf_counter() - t)
+    for X in (DA, DB, DQ, DR):
+        X.destroy()
+    line = {"metric": "elementwise suite HBM GB/s (256-bit add)", "value": res["add"]["gbs"], "unit": "GB/s",
+            "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res["add"]["ms"], "dtype": "u32", "data": "synthetic (seeded splitmix64 limbs)",
+            "config": {"workload": "2^22 x 256-bit elementwise ops, 2^18 x 512x512 mul, 2^18 x 2048/1024 divmod",
+                       "l2": "working sets above the 126 MB L2"},
+            "roofline": {"bound": "hbm", "peak": hbm, "unit": "GB/s", "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
+            "imad_peak_timad_s": imad_peak, "ops": res,
+            "cpu_baseline": {"ops_per_s": cpu, "cores": orc.max_threads(), "kind": "port",
+                             "sample": "full arrays, GMP mpz under OpenMP"},
+            "result_check": all(r["check"] for r in res.values())}
+    print(json.dumps(line), flush=True)
+    h.destroy()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -448,12 +675,21 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true")
-    ap.add_argument("--workload", default="powm2048", choices=["powm2048", "mixed"])
+    ap.add_argument("--workload", default="powm2048", choices=["powm2048", "mixed", "serve", "elementwise"])
+    ap.add_argument("--serve-seconds", type=float, default=1.0)
+    ap.add_argument("--serve-peak-requests", type=int, default=3000)
+    ap.add_argument("--serve-sync-requests", type=int, default=40)
     ap.add_argument("--crt", type=int, default=16384)
     ap.add_argument("--crt-keys", type=int, default=256)
     args = ap.parse_args()
     if args.workload == "mixed":
         run_mixed(args)
+        return
+    if args.workload == "serve":
+        run_serve(args)
+        return
+    if args.workload == "elementwise":
+        run_elementwise(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

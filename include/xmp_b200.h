@@ -148,6 +148,72 @@ xmpError_t XMPAPI xmpSelectorPredict(xmpHandle_t handle, const float *params, co
  * log2 exponent length) and the per-call choice becomes a table lookup. */
 xmpError_t XMPAPI xmpSelectorLoad(xmpHandle_t handle, const float *params);
 
+/* ---- serving loop ----------------------------------------------------------
+ * No counterpart in the reference.  A server admits modular-exponentiation
+ * requests (1 .. max_wave_ops ops under one registered key) from any thread
+ * and serves them with continuous batching: whenever one of its launch
+ * streams is idle, a scheduler thread launches the pending requests of a
+ * precision class (oldest first) as one wave, so requests that arrive while
+ * others run start as soon as a stream and op slots free up and overlap with
+ * them on the device, and waves grow with the load.  Each wave's kernel
+ * configuration follows the class's ops in flight: latency-optimal when the
+ * GPU is quiet, throughput-optimal when it is full.  Keys (odd moduli) and their
+ * Montgomery constants stay on the device; op slots and window tables come
+ * from a fixed device arena sized by the HBM budget, which is the admission
+ * limit.  Operands and results are host rows of precision/32 little-endian
+ * 32-bit limbs per op (exponents have the modulus's precision); results are
+ * bit-identical to xmpIntegersPowm on the same operands. */
+typedef struct _xmpServer_t *xmpServer_t;
+
+typedef struct {
+  size_t hbm_budget;      /* device bytes for keys, op slots and window tables (0: 8 GiB) */
+  uint32_t max_wave_ops;  /* ops per launch wave, and per request (0: 4096) */
+  uint32_t streams;       /* launch streams, i.e. waves in flight at most (0: 32; give the process
+                             CUDA_DEVICE_MAX_CONNECTIONS >= streams so they map to separate
+                             hardware queues) */
+  uint32_t max_keys;      /* key capacity per precision class (0: 4096) */
+  uint32_t max_slots;     /* op slots per class, at most (0: 262144; fewer if the budget says so) */
+} xmpServerConfig_t;
+
+typedef struct {
+  uint64_t requests_submitted;
+  uint64_t requests_completed;
+  uint64_t ops_completed;
+  uint64_t waves;             /* launch waves */
+  uint64_t admission_stalls;  /* times a class had ready work but no free op slots */
+  uint32_t max_inflight_ops;
+  uint32_t classes;
+  size_t device_bytes;        /* device memory the server holds */
+} xmpServerStats_t;
+
+/* One precision class per entry of `precisions` (multiples of 32 bits).  The
+ * handle provides the device, allocators and tuner (choices are fixed at
+ * creation); it must outlive the server. */
+xmpError_t XMPAPI xmpServerCreate(xmpHandle_t handle, const uint32_t *precisions, uint32_t n_classes,
+                                  const xmpServerConfig_t *config, xmpServer_t *server);
+xmpError_t XMPAPI xmpServerDestroy(xmpServer_t server);
+/* Registers `count` odd moduli (host rows) and computes R^2 mod m on the
+ * device; key ids are first_key .. first_key+count-1. */
+xmpError_t XMPAPI xmpServerAddKeys(xmpServer_t server, uint32_t precision, const uint32_t *moduli, uint32_t count,
+                                   uint32_t *first_key);
+/* Queues out[i] = bases[i]^exps[i] mod key for i < nops.  The buffers must
+ * stay valid until the request is reported done. */
+xmpError_t XMPAPI xmpServerSubmit(xmpServer_t server, uint32_t key, uint32_t nops, const uint32_t *bases,
+                                  const uint32_t *exps, uint32_t *out, uint64_t *request);
+/* Waits up to timeout_us (0: poll) for a request; *done = 1 once its results
+ * are in `out` (the request id is then retired). */
+xmpError_t XMPAPI xmpServerWait(xmpServer_t server, uint64_t request, uint32_t timeout_us, int32_t *done);
+xmpError_t XMPAPI xmpServerStats(xmpServer_t server, xmpServerStats_t *stats);
+/* Open-loop replay of n requests arriving at arrival_ns (non-decreasing, from
+ * the start): mode 0 through the server, mode 1 as plain synchronous
+ * per-request calls (Import, xmpIntegersPowm, Export) on the calling thread.
+ * latency_ns[i] = completion - scheduled arrival; seconds = last completion
+ * - start.  The server must be idle. */
+xmpError_t XMPAPI xmpServerReplay(xmpServer_t server, uint32_t n, const uint32_t *keys, const uint32_t *nops,
+                                  const uint64_t *arrival_ns, const uint32_t *const *bases,
+                                  const uint32_t *const *exps, uint32_t *const *outs, int32_t mode,
+                                  uint64_t *latency_ns, double *seconds);
+
 #ifdef __cplusplus
 }
 #endif

@@ -38,10 +38,11 @@ def test_python_binding_covers_api():
         set(xmp_b200.API_NAMES) | {"xmpHandleCreateWithMemoryFunctions", "xmpHandleGetMemoryFunctions"}
 
 
+@pytest.mark.parametrize("header", ["xmp.h", "xmp_b200.h"])
 @pytest.mark.parametrize("lang,compiler", [("c", "gcc"), ("c++", "g++")])
-def test_header_compiles(tmp_path, lang, compiler):
+def test_header_compiles(tmp_path, lang, compiler, header):
     src = tmp_path / ("t." + ("c" if lang == "c" else "cc"))
-    src.write_text('#include "xmp.h"\nint main(void){ xmpHandle_t h; (void)h; return xmpErrorSuccess; }\n')
+    src.write_text('#include "%s"\nint main(void){ xmpHandle_t h; (void)h; return xmpErrorSuccess; }\n' % header)
     p = subprocess.run([compiler, "-x", lang, "-c", str(src), "-I", os.path.join(ROOT, "include"), "-I",
                         "/usr/local/cuda/include", "-o", str(tmp_path / "t.o")], capture_output=True, text=True)
     assert p.returncode == 0, p.stderr

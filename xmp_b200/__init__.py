@@ -102,6 +102,13 @@ _SIGS = {
     "xmpPowmBatchPlanExecute": [_VP, _VP],
     "xmpPowmBatchPlanDestroy": [_VP, _VP],
     "xmpPowmBatchPlanInfo": [_VP, ctypes.POINTER(_I32), _VP, _VP, _VP, _VP, _I32],
+    "xmpServerCreate": [_VP, _VP, _U32, _VP, ctypes.POINTER(_VP)],
+    "xmpServerDestroy": [_VP],
+    "xmpServerAddKeys": [_VP, _U32, _VP, _U32, ctypes.POINTER(_U32)],
+    "xmpServerSubmit": [_VP, _U32, _U32, _VP, _VP, _VP, ctypes.POINTER(ctypes.c_uint64)],
+    "xmpServerWait": [_VP, ctypes.c_uint64, _U32, ctypes.POINTER(_I32)],
+    "xmpServerStats": [_VP, _VP],
+    "xmpServerReplay": [_VP, _U32, _VP, _VP, _VP, _VP, _VP, _VP, _I32, _VP, ctypes.POINTER(ctypes.c_double)],
 }
 for _n in ("Add", "Sub", "Mul", "Div", "Mod", "Ior", "And", "Xor"):
     _SIGS["xmpIntegers" + _n] = [_VP, _VP, _VP, _VP, _U32]
@@ -355,6 +362,86 @@ class BatchPlan:
         if self.p:
             check(lib().xmpPowmBatchPlanDestroy(self.h.h, self.p), "xmpPowmBatchPlanDestroy")
             self.p = None
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_size_t), ("max_wave_ops", _U32), ("streams", _U32), ("max_keys", _U32),
+                ("max_slots", _U32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("requests_submitted", ctypes.c_uint64), ("requests_completed", ctypes.c_uint64),
+                ("ops_completed", ctypes.c_uint64), ("waves", ctypes.c_uint64),
+                ("admission_stalls", ctypes.c_uint64), ("max_inflight_ops", _U32), ("classes", _U32),
+                ("device_bytes", ctypes.c_size_t)]
+
+
+class Server:
+    """Continuous-batching modexp server (xmpServer_t).  Operand and result
+    buffers are numpy uint32 arrays of shape (nops, precision / 32)."""
+
+    def __init__(self, h, precisions, **config):
+        self.h = h
+        cfg = ServerConfig(**config)
+        prec = (_U32 * len(precisions))(*precisions)
+        p = _VP()
+        check(lib().xmpServerCreate(h.h, prec, len(precisions), ctypes.byref(cfg), ctypes.byref(p)),
+              "xmpServerCreate")
+        self.s = p
+        self._keep = {}
+
+    def add_keys(self, precision, moduli):
+        m = np.ascontiguousarray(moduli, dtype=np.uint32)
+        first = _U32(0)
+        check(lib().xmpServerAddKeys(self.s, precision, _ptr(m), m.shape[0], ctypes.byref(first)),
+              "xmpServerAddKeys")
+        return first.value
+
+    def submit(self, key, bases, exps, out):
+        """Queues out = bases^exps mod key (row-wise); returns the request id.
+        The arrays are kept alive until wait() reports the request done."""
+        b = np.ascontiguousarray(bases, dtype=np.uint32)
+        e = np.ascontiguousarray(exps, dtype=np.uint32)
+        assert out.flags.c_contiguous and out.dtype == np.uint32 and out.shape == b.shape
+        rid = ctypes.c_uint64(0)
+        check(lib().xmpServerSubmit(self.s, key, b.shape[0], _ptr(b), _ptr(e), _ptr(out), ctypes.byref(rid)),
+              "xmpServerSubmit")
+        self._keep[rid.value] = (b, e, out)
+        return rid.value
+
+    def wait(self, request, timeout_us=10_000_000):
+        done = _I32(0)
+        check(lib().xmpServerWait(self.s, request, timeout_us, ctypes.byref(done)), "xmpServerWait")
+        if done.value:
+            self._keep.pop(request, None)
+        return bool(done.value)
+
+    def stats(self):
+        st = ServerStats()
+        check(lib().xmpServerStats(self.s, ctypes.byref(st)), "xmpServerStats")
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+
+    def replay(self, keys, arrival_ns, bases, exps, outs, mode=0):
+        """Open-loop replay; bases/exps/outs are lists of (nops, n) arrays.
+        Returns (latency_ns array, seconds)."""
+        n = len(keys)
+        k = np.ascontiguousarray(keys, dtype=np.uint32)
+        nops = np.array([b.shape[0] for b in bases], dtype=np.uint32)
+        arr = np.ascontiguousarray(arrival_ns, dtype=np.uint64)
+        bp = (ctypes.c_void_p * n)(*[b.ctypes.data for b in bases])
+        ep = (ctypes.c_void_p * n)(*[e.ctypes.data for e in exps])
+        op = (ctypes.c_void_p * n)(*[o.ctypes.data for o in outs])
+        lat = np.zeros(n, dtype=np.uint64)
+        secs = ctypes.c_double(0)
+        check(lib().xmpServerReplay(self.s, n, _ptr(k), _ptr(nops), _ptr(arr), bp, ep, op, mode, _ptr(lat),
+                                    ctypes.byref(secs)), "xmpServerReplay")
+        return lat, secs.value
+
+    def destroy(self):
+        if self.s:
+            check(lib().xmpServerDestroy(self.s), "xmpServerDestroy")
+            self.s = None
+            self._keep.clear()
 
 
 def powm(h, out, base, exp, mod_, count, asynchronous=False):

@@ -238,6 +238,8 @@ def main():
     c.add_argument("--out", default=DEFAULT_DATA)
     c.add_argument("--max-ms", type=float, default=25.0)
     c.add_argument("--reps", type=int, default=1)
+    c.add_argument("--append", default=None,
+                   help="existing dataset: only shapes it lacks are timed, the result is the union")
     t = sub.add_parser("train")
     t.add_argument("--data", default=DEFAULT_DATA)
     t.add_argument("--out", default=DEFAULT_WEIGHTS)
@@ -251,8 +253,15 @@ def main():
     h = xmp.Handle()
     if a.cmd == "collect":
         shapes = grid(a.max_ms)
+        meta = {"device": torch.cuda.get_device_name(0), "reps": a.reps, "max_ms": a.max_ms}
+        old_shapes, old_ms = [], np.zeros((0, NCAND), dtype=np.float32)
+        if a.append:
+            old_shapes, old_ms, old_meta = load_dataset(a.append)
+            meta["appended_to"] = old_meta
+            have = set(old_shapes)
+            shapes = [s for s in shapes if s not in have]
         ms = collect(h, shapes, a.reps, log=lambda s: print(s, flush=True))
-        save_dataset(a.out, shapes, ms, {"device": torch.cuda.get_device_name(0), "reps": a.reps})
+        save_dataset(a.out, list(old_shapes) + list(shapes), np.concatenate([old_ms, ms]), meta)
     else:
         shapes, ms, meta = load_dataset(a.data)
         tr, te, held = split_cells(shapes)
