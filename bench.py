@@ -49,6 +49,25 @@ def imad_per_modexp(bits, ebits):
     return (ebits + math.ceil(ebits / 5)) * (4 * n * n + n)
 
 
+def replica_seed(rank):
+    """Each replica (rank) works on its own seeded batch: no data is shared, so
+    the ranks need no collective beyond the timing barrier and reduction."""
+    return 2048 + 7919 * rank
+
+
+def aggregate_over_ranks(dist, local_ms, device, instances_per_rank, steps, world):
+    """Whole-job throughput from per-rank elapsed times: the max over ranks
+    (the job ends when its slowest replica does) and every rank's instances.
+    Returns (max_ms, instances per second)."""
+    ms = local_ms
+    if dist is not None:
+        import torch
+        t = torch.tensor([local_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, world * instances_per_rank * steps / (ms * 1e-3)
+
+
 def make_inputs(bits, count, seed=2048):
     import oracle as orc  # seeded generators only
     n = bits // 32
@@ -110,6 +129,17 @@ class ClockSampler:
         loaded = [s for s in sm if mx and s > 0.5 * mx] or sm
         return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": mx,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def profiled_traffic(bits, count):
+    """DRAM bytes per powm launch from a committed ncu capture of this exact workload
+    (dram__bytes_read.sum + dram__bytes_write.sum), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "powm_kernel_%dbit_traffic.json" % bits)) as f:
+            d = json.load(f)
+    except (OSError, ValueError):
+        return None
+    return d.get("dram_bytes_per_launch") if d.get("instances") == count else None
 
 
 def probe_imad_peak():
@@ -180,7 +210,7 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     bits, count = args.bits, args.count
     n = bits // 32
-    x, e, m = make_inputs(bits, count, seed=2048 + 7919 * rank)
+    x, e, m = make_inputs(bits, count, seed=replica_seed(rank))
 
     h = xmp.Handle()
     h.set_stream(stream.cuda_stream)
@@ -218,12 +248,7 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     clocks = sampler.stop() if sampler else None
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * count * args.steps / (total_ms * 1e-3)
+    total_ms, value = aggregate_over_ranks(dist, sum(step_ms), "cuda", count, args.steps, world)
 
     # ---- end-to-end through the C API with pinned host buffers ----
     hx = torch.from_numpy(x).pin_memory()
@@ -250,12 +275,7 @@ def run_ours(args, rank, world, local_rank):
         e2e_step()
     b.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = a.elapsed_time(b)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * count * args.steps / (e2e_ms * 1e-3)
+    e2e_ms, e2e_value = aggregate_over_ranks(dist, a.elapsed_time(b), "cuda", count, args.steps, world)
 
     # result check on a sample against the oracle (outside every timed region)
     res = hout.numpy().view(np.uint32)
@@ -273,7 +293,7 @@ def run_ours(args, rank, world, local_rank):
     kernel_s = statistics.median(step_ms) * 1e-3
     achieved = algo / kernel_s / 1e12
     roofline = {"bound": "imad", "achieved": achieved, "peak": peaks["imad"], "unit": "TIMAD/s",
-                "frac": achieved / peaks["imad"], "traffic": None,
+                "frac": achieved / peaks["imad"], "traffic": profiled_traffic(bits, count),
                 "peak_source": "measured live: libxmpprobe independent mad.lo.u32 chains, all SMs",
                 "carry_row_peak": peaks["carry_rows"],
                 "algorithmic_imad_per_modexp": imad_per_modexp(bits, bits)}
@@ -281,8 +301,10 @@ def run_ours(args, rank, world, local_rank):
     cpu = None
     if not args.no_cpu:
         rate, used, sample, dt = cpu_gmp_rate(x, e, m, target_s=args.cpu_seconds)
+        rate1, _, sample1, dt1 = cpu_gmp_rate(x, e, m, target_s=max(1.0, args.cpu_seconds / 4), threads=1)
         cpu = {"value": rate, "unit": "modexp/s", "cores": used, "kind": "port",
-               "sample": "%d instances of the same workload (%.1f s, GMP mpz_powm via OpenMP)" % (sample, dt)}
+               "sample": "%d instances of the same workload (%.1f s, GMP mpz_powm via OpenMP)" % (sample, dt),
+               "single_core": {"value": rate1, "sample": "%d instances (%.1f s, 1 thread)" % (sample1, dt1)}}
 
     line = {
         "metric": "%d-bit modexp/s" % bits, "value": value, "unit": "modexp/s", "n_gpus": world,
@@ -575,19 +597,25 @@ def run_elementwise(args):
     SH = torch.from_numpy(sh).cuda()
     I32 = torch.empty(E, dtype=torch.int32, device="cuda")
 
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
+
     def timed(fn):
+        """Median device time of one call.  Every step is queued behind an L2
+        flush (a 252 MB write), so the GPU never waits for the host inside the
+        events and no step finds its operands in L2; one synchronize at the end."""
         for _ in range(args.warmup):
             fn()
         torch.cuda.synchronize()
-        ts = []
+        evs = []
         for _ in range(args.steps):
+            flush.zero_()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             fn()
             e1.record(stream)
-            torch.cuda.synchronize()
-            ts.append(e0.elapsed_time(e1))
-        return statistics.median(ts)
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        return statistics.median([e0.elapsed_time(e1) for e0, e1 in evs])
 
     S = 4096
     res = {}
@@ -653,7 +681,7 @@ def run_elementwise(args):
             "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": res["add"]["ms"], "dtype": "u32", "data": "synthetic (seeded splitmix64 limbs)",
             "config": {"workload": "2^22 x 256-bit elementwise ops, 2^18 x 512x512 mul, 2^18 x 2048/1024 divmod",
-                       "l2": "working sets above the 126 MB L2"},
+                       "l2": "flushed before every step (252 MB write, queued ahead of the events)"},
             "roofline": {"bound": "hbm", "peak": hbm, "unit": "GB/s", "peak_source": "MEASURED_PEAKS.json hbm_gbs"},
             "imad_peak_timad_s": imad_peak, "ops": res,
             "cpu_baseline": {"ops_per_s": cpu, "cores": orc.max_threads(), "kind": "port",
