@@ -514,9 +514,13 @@ def run_serve(args):
         keys, arr, bases, exps, outs, ops, ks, nops = stream(n_req, rate)
         lat, secs = srv.replay(keys, arr, bases, exps, outs, mode=mode)
         ms = lat.astype(np.float64) * 1e-6
+        bits = np.array([blocks[k][5] for k in ks])
+        by_bits = {int(b): {"p50_ms": float(np.percentile(ms[bits == b], 50)),
+                            "p99_ms": float(np.percentile(ms[bits == b], 99))}
+                   for b in sorted(set(bits.tolist()))}
         return {"offered_ops_per_s": rate, "requests": n_req, "ops": ops, "ops_per_s": ops / secs,
                 "p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
-                "p999_ms": float(np.percentile(ms, 99.9)), "max_ms": float(ms.max())}, ks, nops
+                "p999_ms": float(np.percentile(ms, 99.9)), "max_ms": float(ms.max()), "by_bits": by_bits}, ks, nops
 
     # latency floor: one op alone per size (median of 3)
     floor = {}

@@ -117,7 +117,10 @@ xmpError_t XMPAPI xmpTuneMeasure(xmpHandle_t handle, const xmpTuneShape_t *shape
 
 /* Records / queries the handle's choice for a shape.  Lookup order: a choice
  * set for the exact shape, else the loaded selector's table, else the
- * built-in heuristic (source 1, 2, 0). */
+ * built-in heuristic (source 1, 2, 0).  A new handle starts with the
+ * selector compiled into the library (trained on this library's B200
+ * timings) loaded; xmpTuneClear drops every choice and the selector, leaving
+ * the heuristic. */
 xmpError_t XMPAPI xmpTuneSetChoice(xmpHandle_t handle, const xmpTuneShape_t *shape, int32_t slot);
 xmpError_t XMPAPI xmpTuneGetChoice(xmpHandle_t handle, const xmpTuneShape_t *shape, int32_t *slot, int32_t *source);
 xmpError_t XMPAPI xmpTuneClear(xmpHandle_t handle);

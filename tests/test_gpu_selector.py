@@ -102,7 +102,7 @@ def test_selector_table_lookup(handle):
             assert valid[slot.value]
             # the grid cell's representative point (geometric middle of its count / exponent
             # buckets) predicts this slot as the best valid one
-            cb = int(np.floor(np.log2(sh[3])))
+            cb = max(int(np.floor(np.log2(sh[3]))), 6)  # batches below 2^6 take the 2^6 cell
             eb = int(np.floor(np.log2(max(sh[2], 1))))
             x = np.array([[sh[0] - 1.0, (np.log2(sh[1]) - 10.0) / 4.0, (cb + 0.5 - 13.0) / 7.0,
                            (eb + 0.5 - 7.0) / 7.0 if sh[0] == 2 else -1.0]])

@@ -35,7 +35,7 @@ def _rank(rank, world, port, out):
 
 def test_two_replicas_gloo():
     world = 2
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.spawn(_rank, args=(world, _free_port(), out), nprocs=world, join=True)
         res = dict(out)

@@ -102,6 +102,38 @@ struct ShiftedDividend {
   }
 };
 
+// Limbs of one instance read through a one-group cache: walking the limbs up
+// or down loads each 128-bit group once instead of one 4-byte word per limb.
+struct LimbCursor {
+  const ArrayView *a;
+  uint32_t e;
+  int32_t g;
+  uint4 v;
+  __device__ __forceinline__ uint32_t operator()(int32_t j) {
+    if (j < 0 || j >= (int32_t)a->nlimbs) return 0u;
+    const int32_t gg = j >> 2;
+    if (gg != g) {
+      v = load_group(a->limbs, a->nlimbs, a->stride, e, (uint32_t)gg);
+      g = gg;
+    }
+    const uint32_t r = j & 3;
+    return r == 0 ? v.x : r == 1 ? v.y : r == 2 ? v.z : v.w;
+  }
+};
+
+// limb t of a * 2^(32z + s), through two cursors (the limb and the one below it)
+struct ShiftedCursor {
+  LimbCursor hi, lo;
+  int32_t z;
+  uint32_t s;
+  __device__ __forceinline__ uint32_t operator()(int32_t t) {
+    const int32_t j = t - z;
+    const uint32_t h = hi(j);
+    if (s == 0) return h;
+    return (h << s) | (lo(j - 1) >> (32 - s));
+  }
+};
+
 __device__ __forceinline__ void write_limb(const OutView &o, uint32_t e, uint32_t j, uint32_t v) {
   if (j < o.nlimbs) limb_ref(o.limbs, o.stride, e, j) = v;
 }
@@ -158,22 +190,28 @@ __global__ void __launch_bounds__(256) divmod_reg_kernel(DivArgs d) {
     for (int k = 0; k < BN; k++) V[k] = sb(k);
   }
   const uint32_t v = reciprocal_2by1(V[BN - 1]);
-  ShiftedDividend sa{&d.a, ea, z, s};
+  ShiftedCursor sa{LimbCursor{&d.a, ea, -1, make_uint4(0, 0, 0, 0)}, LimbCursor{&d.a, ea, -1, make_uint4(0, 0, 0, 0)},
+                   z, s};
   uint32_t W[BN + 1];
 #pragma unroll
   for (int k = 0; k <= BN; k++) W[k] = sa(m + k);
 
+  // quotient limbs collect in a group buffer and are stored 128 bits at a time
+  uint32_t qb0 = 0, qb1 = 0, qb2 = 0, qb3 = 0;
   for (int32_t j = m; j >= 0; j--) {
     uint32_t qh = estimate_q(W[BN], W[BN - 1], BN >= 2 ? W[BN >= 2 ? BN - 2 : 0] : 0u, V[BN - 1],
                              BN >= 2 ? V[BN >= 2 ? BN - 2 : 0] : 0u, v, BN >= 2);
-    // W -= qh * V: low halves at limbs 0..BN-1, high halves at 1..BN.
-    W[0] = sub_cc(W[0], qh * V[0]);
+    // W -= qh * V: one mul.wide per limb; low halves at limbs 0..BN-1, high halves at 1..BN.
+    uint64_t p[BN];
 #pragma unroll
-    for (int k = 1; k < BN; k++) W[k] = subc_cc(W[k], qh * V[k]);
+    for (int k = 0; k < BN; k++) p[k] = mul_wide(qh, V[k]);
+    W[0] = sub_cc(W[0], (uint32_t)p[0]);
+#pragma unroll
+    for (int k = 1; k < BN; k++) W[k] = subc_cc(W[k], (uint32_t)p[k]);
     W[BN] = subc(W[BN], 0u);
-    W[1] = sub_cc(W[1], __umulhi(qh, V[0]));
+    W[1] = sub_cc(W[1], (uint32_t)(p[0] >> 32));
 #pragma unroll
-    for (int k = 2; k <= BN; k++) W[k] = subc_cc(W[k], __umulhi(qh, V[k - 1]));
+    for (int k = 2; k <= BN; k++) W[k] = subc_cc(W[k], (uint32_t)(p[k - 1] >> 32));
     if (W[BN] != 0) {  // estimate was one too large: add back
       qh--;
       W[0] = add_cc(W[0], V[0]);
@@ -181,26 +219,54 @@ __global__ void __launch_bounds__(256) divmod_reg_kernel(DivArgs d) {
       for (int k = 1; k < BN; k++) W[k] = addc_cc(W[k], V[k]);
       W[BN] = addc(W[BN], 0u);
     }
-    if (d.q.limbs) write_limb(d.q, eqo, (uint32_t)j, qh);
+    const uint32_t r4 = (uint32_t)j & 3u;
+    qb0 = r4 == 0 ? qh : qb0;
+    qb1 = r4 == 1 ? qh : qb1;
+    qb2 = r4 == 2 ? qh : qb2;
+    qb3 = r4 == 3 ? qh : qb3;
+    if (r4 == 0) {
+      const uint32_t g = (uint32_t)j >> 2;
+      if (d.q.limbs && g * 4 < d.q.nlimbs) store_group(d.q.limbs, d.q.nlimbs, d.q.stride, eqo, g, make_uint4(qb0, qb1, qb2, qb3));
+      qb0 = qb1 = qb2 = qb3 = 0;
+    }
     if (j > 0) {
 #pragma unroll
       for (int k = BN; k > 0; k--) W[k] = W[k - 1];
       W[0] = sa(j - 1);
     }
   }
-  if (d.q.limbs) zero_limbs(d.q, eqo, (uint32_t)(m + 1));
+  // limbs above the quotient's top group
+  if (d.q.limbs) zero_limbs(d.q, eqo, (uint32_t)(m / 4 + 1) * 4);
   if (d.r.limbs) {
     // remainder = W >> S
+    if (z == 0) {
+      const uint32_t rg = div_up(d.r.nlimbs, 4);
 #pragma unroll
-    for (int k = 0; k < BN; k++) {
-      int32_t dst = k - z;
-      if (dst >= 0) {
-        uint32_t hi = (k + 1 < BN) ? W[k + 1 < BN ? k + 1 : 0] : 0u;
-        uint32_t val = s ? ((W[k] >> s) | (hi << (32 - s))) : W[k];
-        write_limb(d.r, ero, (uint32_t)dst, val);
+      for (int g = 0; g < (BN + 3) / 4; g++) {
+        uint32_t o[4];
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+          const int k = 4 * g + t;
+          const uint32_t lo = k < BN ? W[k < BN ? k : 0] : 0u;
+          const uint32_t hi = (k + 1 < BN) ? W[k + 1 < BN ? k + 1 : 0] : 0u;
+          o[t] = s ? ((lo >> s) | (hi << (32 - s))) : lo;
+        }
+        if ((uint32_t)g < rg) store_group(d.r.limbs, d.r.nlimbs, d.r.stride, ero, g, make_uint4(o[0], o[1], o[2], o[3]));
       }
+      for (uint32_t g = (BN + 3) / 4; g < rg; g++)
+        store_group(d.r.limbs, d.r.nlimbs, d.r.stride, ero, g, make_uint4(0, 0, 0, 0));
+    } else {
+#pragma unroll
+      for (int k = 0; k < BN; k++) {
+        int32_t dst = k - z;
+        if (dst >= 0) {
+          uint32_t hi = (k + 1 < BN) ? W[k + 1 < BN ? k + 1 : 0] : 0u;
+          uint32_t val = s ? ((W[k] >> s) | (hi << (32 - s))) : W[k];
+          write_limb(d.r, ero, (uint32_t)dst, val);
+        }
+      }
+      zero_limbs(d.r, ero, (uint32_t)(BN - z));
     }
-    zero_limbs(d.r, ero, (uint32_t)(BN - z));
   }
 }
 

@@ -101,6 +101,47 @@ __global__ void __launch_bounds__(256) shf_kernel(ArrayView a, OutView c, const 
   }
 }
 
+// Same operation for operands of at most kShfSmemGroups limb groups: the
+// operand is read with coalesced 128-bit group loads into this thread's
+// column of shared memory ([limb][thread], conflict-free), and the shifted
+// limbs are read back from there, so a warp whose lanes shift by different
+// amounts still touches HBM only with whole groups.
+constexpr uint32_t kShfSmemGroups = 8;  // up to 1024-bit operands
+__global__ void __launch_bounds__(256) shf_smem_kernel(ArrayView a, OutView c, const int32_t *shift,
+                                                       uint32_t shift_count, uint32_t count) {
+  extern __shared__ uint32_t col[];  // [4 * groups of a][256]
+  const uint32_t tid = threadIdx.x;
+  uint32_t i = blockIdx.x * blockDim.x + tid;
+  if (i >= count) return;
+  uint32_t ea = in_element(a, i), ec = out_element(c, i);
+  if (ec >= c.count) return;
+  const uint32_t ag = div_up(a.nlimbs, 4);
+  for (uint32_t g = 0; g < ag; g++) {
+    uint4 v = load_group(a.limbs, a.nlimbs, a.stride, ea, g);
+    col[(4 * g) * 256 + tid] = v.x;
+    col[(4 * g + 1) * 256 + tid] = v.y;
+    col[(4 * g + 2) * 256 + tid] = v.z;
+    col[(4 * g + 3) * 256 + tid] = v.w;
+  }
+  int64_t t = -(int64_t)shift[i % shift_count];
+  int64_t q = (t >= 0) ? t / 32 : -((-t + 31) / 32);  // floor(t / 32)
+  uint32_t r = (uint32_t)(t - q * 32);
+  const int64_t na = a.nlimbs;
+  auto limb_at = [&](int64_t j) -> uint32_t { return (j < 0 || j >= na) ? 0u : col[j * 256 + tid]; };
+  const uint32_t groups = div_up(c.nlimbs, 4);
+  uint32_t low = limb_at(q);
+  for (uint32_t g = 0; g < groups; g++) {
+    uint32_t out[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      uint32_t high = limb_at(q + (int64_t)(g * 4 + k) + 1);
+      out[k] = r ? __funnelshift_r(low, high, r) : low;
+      low = high;
+    }
+    store_group(c.limbs, c.nlimbs, c.stride, ec, g, make_uint4(out[0], out[1], out[2], out[3]));
+  }
+}
+
 // Compares a and b as unsigned integers of their own precisions.  (The
 // reference tests the longer operand's extra limbs of instance 0 instead of
 // the selected instance, implementations.h:795; here the selected one.)
@@ -126,7 +167,14 @@ __global__ void __launch_bounds__(256) popc_kernel(ArrayView a, uint32_t *out, u
   if (i >= count) return;
   uint32_t ea = in_element(a, i);
   uint32_t groups = div_up(a.nlimbs, 4), s = 0;
-  for (uint32_t g = 0; g < groups; g++) {
+  uint32_t g = 0;
+  for (; g + 2 <= groups; g += 2) {  // two independent group loads in flight per thread
+    uint4 x = load_group(a.limbs, a.nlimbs, a.stride, ea, g);
+    uint4 y = load_group(a.limbs, a.nlimbs, a.stride, ea, g + 1);
+    s += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w) + __popc(y.x) + __popc(y.y) + __popc(y.z) +
+         __popc(y.w);
+  }
+  if (g < groups) {
     uint4 x = load_group(a.limbs, a.nlimbs, a.stride, ea, g);
     s += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
   }
@@ -275,9 +323,15 @@ xmpError_t XMPAPI xmpIntegersShfAsync(xmpHandle_t h, xmpIntegers_t c, const xmpI
   OutTarget t;
   xmpError_t e = begin_output(h, c, c == a, true, &t);
   if (e != xmpErrorSuccess) return e;
-  shf_kernel<<<grid_for(count, 256), 256, 0, h->stream>>>(view_in(a, p->indices[1], p->indices_count[1]),
-                                                           view_out(c, t.limbs, p->indices[0]), dshift, scount,
-                                                           count);
+  if (div_up(a->nlimbs, 4) <= kShfSmemGroups)
+    shf_smem_kernel<<<grid_for(count, 256), 256, div_up(a->nlimbs, 4) * 4 * 256 * sizeof(uint32_t), h->stream>>>(
+        view_in(a, p->indices[1], p->indices_count[1]),
+                                                                  view_out(c, t.limbs, p->indices[0]), dshift,
+                                                                  scount, count);
+  else
+    shf_kernel<<<grid_for(count, 256), 256, 0, h->stream>>>(view_in(a, p->indices[1], p->indices_count[1]),
+                                                             view_out(c, t.limbs, p->indices[0]), dshift, scount,
+                                                             count);
   e = end_output(h, c, t);
   if (e != xmpErrorSuccess) return e;
   return check_cuda();

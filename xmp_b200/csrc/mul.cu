@@ -58,17 +58,28 @@ __global__ void __launch_bounds__(256) mul_reg_kernel(ArrayView a, ArrayView b, 
   load_limbs<BL>(B, b, eb);
 #pragma unroll
   for (int k = 0; k < AL + BL; k++) P[k] = 0;
+  // Row j adds A * B[j] at word j: the AL products are one mul.wide each (the
+  // FMA pipe), folded in by two ALU carry chains -- low halves at j+k, high
+  // halves at j+k+1.  The partial product after row j fits in j+AL+1 words,
+  // so the chains never carry out of P[j+AL].
 #pragma unroll
   for (int j = 0; j < BL; j++) {
-    uint32_t w = B[j];
-    P[j] = mad_lo_cc(A[0], w, P[j]);
+    const uint32_t w = B[j];
+    uint64_t p[AL];
 #pragma unroll
-    for (int k = 1; k < AL; k++) P[j + k] = madc_lo_cc(A[k], w, P[j + k]);
+    for (int k = 0; k < AL; k++) p[k] = mul_wide(A[k], w);
+    P[j] = add_cc(P[j], (uint32_t)p[0]);
+#pragma unroll
+    for (int k = 1; k < AL; k++) P[j + k] = addc_cc(P[j + k], (uint32_t)p[k]);
     P[j + AL] = addc(0u, 0u);
-    P[j + 1] = mad_hi_cc(A[0], w, P[j + 1]);
+    if (AL > 1) {
+      P[j + 1] = add_cc(P[j + 1], (uint32_t)(p[0] >> 32));
 #pragma unroll
-    for (int k = 1; k < AL - 1; k++) P[j + 1 + k] = madc_hi_cc(A[k], w, P[j + 1 + k]);
-    P[j + AL] = madc_hi(A[AL - 1], w, P[j + AL]);
+      for (int k = 1; k < AL - 1; k++) P[j + 1 + k] = addc_cc(P[j + 1 + k], (uint32_t)(p[k] >> 32));
+      P[j + AL] = addc(P[j + AL], (uint32_t)(p[AL - 1] >> 32));
+    } else {
+      P[j + AL] += (uint32_t)(p[0] >> 32);
+    }
   }
   store_limbs<AL + BL>(P, c, ec);
 }

@@ -9,6 +9,7 @@
 // rules, GMP-style (words, order, size, endian, nails) wire format where nails
 // masks the top `nails` bits of every word after the optional byte swap.
 #include "internal.h"
+#include "tune.h"
 #include <stdlib.h>
 #include <string.h>
 
@@ -268,6 +269,14 @@ xmpError_t XMPAPI xmpHandleCreateWithMemoryFunctions(xmpHandle_t *handle, xmpAll
   h->memory_size = prop.totalGlobalMem;
   h->arch = prop.major * 10 + prop.minor;
   h->sm_count = prop.multiProcessorCount;
+  // Configuration choices start from the compiled-in learned selector; if it cannot be
+  // loaded (e.g. the caller's allocator refuses), the built-in heuristic stays in charge.
+  if (const float *params = xmpb::default_selector_params()) {
+    if (xmpSelectorLoad(h, params) != xmpErrorSuccess) {
+      xmpTuneClear(h);
+      cudaGetLastError();  // a refused allocation is not an error of this call
+    }
+  }
   return check_cuda();
 }
 

@@ -106,11 +106,13 @@ __global__ void grid_infer(const float *params, const uint64_t *valid, uint8_t *
     table[c] = 0xff;
     return;
   }
-  // the cell stands for counts in [2^cb, 2^(cb+1)) and exponents in [2^eb, 2^(eb+1)): use the geometric middle
+  // the cell stands for counts in [2^cb, 2^(cb+1)) and exponents in [2^eb, 2^(eb+1)): use the geometric
+  // middle.  Batches smaller than the smallest one the tuner times (2^6) leave the GPU just as idle as
+  // that one, so they take its choice instead of an extrapolation below the data.
   float x[kIn];
   x[0] = (float)op - 1.0f;
   x[1] = (log2f(32.0f * nl) - 10.0f) / 4.0f;
-  x[2] = ((float)cb + 0.5f - 13.0f) / 7.0f;
+  x[2] = (fmaxf((float)cb, (float)kSelectorMinCountLog2) + 0.5f - 13.0f) / 7.0f;
   x[3] = op == xmpTunePowm ? ((float)eb + 0.5f - 7.0f) / 7.0f : (0.0f - 7.0f) / 7.0f;
   float h1[kH], h2[kH];
   for (int j = 0; j < kH; j++) {
@@ -231,6 +233,23 @@ static void init_params(float *p, uint64_t seed) {
   for (int i = 0; i < kH * kH; i++) p[kOffW2 + i] = uni() * sqrtf(6.0f / kH);
   for (int i = 0; i < kH * kOut; i++) p[kOffW3 + i] = uni() * sqrtf(6.0f / kH);
   for (int j = 0; j < kOut; j++) p[kOffB3 + j] = 0.0f;
+}
+
+// The selector trained on this library's own B200 timings, compiled in by
+// the build (xmp_b200/tuning/b200_selector.f32 as exact hex-float literals):
+// every new handle loads it, the way the reference's kernels read their
+// compiled-in tune tables.
+#if __has_include("default_selector.inc")
+#include "default_selector.inc"
+#endif
+
+const float *default_selector_params() {
+#ifdef XMPB_DEFAULT_SELECTOR_COUNT
+  static_assert(XMPB_DEFAULT_SELECTOR_COUNT == kParams, "embedded selector has the wrong shape");
+  return kDefaultSelector;
+#else
+  return nullptr;
+#endif
 }
 
 xmpError_t selector_fill_table(xmpHandle_t h, const float *params, std::vector<uint8_t> *table) {

@@ -120,6 +120,7 @@ struct Class {
   size_t table_words = 0;  // per slot
   PowmConfig cfg[kBuckets];
   const PowmKernelEntry *entry[kBuckets] = {};
+  bool urgent = false;  // the largest precision: its waves bound the latency tail, so they get priority streams
   // scheduler-owned queues
   std::deque<Req *> pending;
   uint32_t pending_ops = 0;
@@ -142,6 +143,7 @@ struct _xmpServer_t {
   std::vector<std::pair<uint32_t, uint32_t>> keys;  // global key -> (class, key within class)
   std::vector<cudaStream_t> streams;
   std::vector<int> stream_waves;
+  std::vector<bool> stream_high;  // created at the device's greatest stream priority
   int next_stream = 0;
   std::vector<cudaEvent_t> event_pool;
   cudaStream_t setup = nullptr;
@@ -248,12 +250,16 @@ static bool launch_wave(xmpServer_t s, Class &c, Wave *w, uint32_t load) {
     for (uint32_t j = 0; j < q->nops; j++) c.pin_key[at + j] = q->key;
   }
   // the stream with the fewest waves in flight (an idle one when there is one),
-  // rotating among equals so consecutive waves land on different streams
+  // of the class's priority when one of those is as free, rotating among
+  // equals so consecutive waves land on different streams
   const int ns = (int)s->streams.size();
-  int si = s->next_stream % ns;
-  for (int j = 1; j < ns; j++) {
+  int si = -1;
+  for (int j = 0; j < ns; j++) {
     const int k = (s->next_stream + j) % ns;
-    if (s->stream_waves[k] < s->stream_waves[si]) si = k;
+    if (si < 0 || s->stream_waves[k] < s->stream_waves[si] ||
+        (s->stream_waves[k] == s->stream_waves[si] && s->stream_high[k] == c.urgent &&
+         s->stream_high[si] != c.urgent))
+      si = k;
   }
   s->next_stream = si + 1;
   cudaStream_t st = s->streams[si];
@@ -554,11 +560,23 @@ xmpError_t XMPAPI xmpServerCreate(xmpHandle_t h, const uint32_t *precisions, uin
   }
   // ---- streams and the scheduler ----
   if (cudaStreamCreateWithFlags(&s->setup, cudaStreamNonBlocking) != cudaSuccess) return fail(xmpErrorCuda);
+  // Half of the streams at the device's greatest priority: the block scheduler
+  // gives their CTAs the SMs first, and the largest class (whose operations
+  // take longest and so set the latency tail) launches there by preference.
+  int prio_low = 0, prio_high = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+  uint32_t biggest = 0;
+  for (uint32_t i = 1; i < n_classes; i++)
+    if (s->classes[i].precision > s->classes[biggest].precision) biggest = i;
+  if (n_classes > 1) s->classes[biggest].urgent = true;
   for (uint32_t i = 0; i < cf.streams; i++) {
     cudaStream_t st;
-    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return fail(xmpErrorCuda);
+    const bool high = n_classes > 1 && i % 2 == 0;
+    if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, high ? prio_high : prio_low) != cudaSuccess)
+      return fail(xmpErrorCuda);
     s->streams.push_back(st);
     s->stream_waves.push_back(0);
+    s->stream_high.push_back(high);
   }
   s->stats.classes = n_classes;
   s->stats.device_bytes = s->device_bytes;

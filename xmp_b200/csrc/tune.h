@@ -18,6 +18,7 @@ constexpr int kElemSlots = 8;          // {register, streamed} x {32, 64, 128, 2
 constexpr int kGridMaxLimbs = 512;     // selector lookup grid: precisions 32..16384 bits
 constexpr int kGridCountBuckets = 27;  // floor(log2 count), 0..26
 constexpr int kGridExpBuckets = 15;    // floor(log2 exp_bits), 0..14 (powm only)
+constexpr int kSelectorMinCountLog2 = 6;  // smallest batch the tuner times (2^6); smaller batches use its cell
 
 struct ElemConfig {
   int variant = 0;   // 0 register kernel, 1 streamed kernel
@@ -52,6 +53,8 @@ xmpError_t divmod_entry(xmpHandle_t h, xmpIntegers_t q, xmpIntegers_t r, xmpInte
 
 // Selector grid evaluation (selector.cu): fills table[op][limbs-1][cb][eb] with argmin slots.
 xmpError_t selector_fill_table(xmpHandle_t h, const float *params, std::vector<uint8_t> *table);
+// The compiled-in selector parameters (nullptr when the library was built without them).
+const float *default_selector_params();
 size_t grid_index(int op, uint32_t nlimbs, int count_bucket, int exp_bucket);
 int count_bucket(uint32_t count);
 int exp_bucket(uint32_t exp_bits);
