@@ -404,10 +404,8 @@ def run_mixed(args):
         xmp.check(L.xmpIntegersMulAsync(h.h, tmp["f"].x, ka["q"].x, tmp["hh"].x, ncrt))
         xmp.check(L.xmpIntegersAddAsync(h.h, outs[0].x, tmp["f"].x, tmp["mq"].x, ncrt))
 
-    # autotuned batch plan (learned selector installed when its weights exist), replayed as a graph
+    # autotuned batch plan, replayed as a graph (every handle starts with the compiled-in selector)
     selector = os.path.exists(tuning.DEFAULT_WEIGHTS)
-    if selector:
-        tuning.install(h, tuning.load_weights())
     plan = xmp.BatchPlan(h, [(g["O2"], g["X"], g["E"], g["M"], g["count"]) for g in groups],
                          [(outs[1], C, ka["p"], ka["q"], ka["dp"], ka["dq"], ka["qinv"], ncrt)], use_graph=True)
 
@@ -425,8 +423,7 @@ def run_mixed(args):
             ts.append(a.elapsed_time(b))
         return float(np.median(ts))
 
-    # plain launches run with the built-in heuristic only (no tuned entries)
-    xmp.check(xmp.lib().xmpTuneClear(h.h))
+    # plain launches use the library's default choices (the compiled-in selector), as any caller gets
     t_plain = timed(plain, args.steps, args.warmup)
     t_batch = timed(plan.execute, args.steps, args.warmup)
     # the plain launches one at a time: their sum bounds what any schedule of the same kernels can gain
@@ -472,10 +469,8 @@ def run_serve(args):
     import xmp_b200 as xmp
     from xmp_b200 import tuning
     torch.cuda.set_device(0)
-    h = xmp.Handle()
+    h = xmp.Handle()  # starts with the compiled-in selector
     selector = os.path.exists(tuning.DEFAULT_WEIGHTS)
-    if selector:
-        tuning.install(h, tuning.load_weights())
     classes = [(2048, 512), (3072, 307), (4096, 205)]
     srv = xmp.Server(h, [c for c, _ in classes], hbm_budget=8 << 30, max_keys=512)
     # per class: one block of 64 ops per key (bases below that key); a request
@@ -647,6 +642,19 @@ def run_elementwise(args):
     row("cmp", ms, 68, E, np.array_equal(I32[:S].cpu().numpy(), orc.cmp(a[:S], b[:S], S)))
     ms = timed(lambda: xmp.check(L.xmpIntegersPopcAsync(h.h, I32.data_ptr(), A.x, E)))
     row("popc", ms, 36, E, np.array_equal(I32[:S].cpu().numpy().view(np.uint32), orc.popc(a[:S], S)))
+    # add through index arrays (random permutations gathering a and b, scattering c): 96 B of
+    # operands plus three 4-byte indices per op
+    perms = [np.random.default_rng(60 + k).permutation(E).astype(np.uint32) for k in range(3)]
+    pol = xmp.Policy(h)
+    for k in range(3):
+        pol.set_indices(k, perms[k])
+    h.set_policy(pol)
+    ms = timed(lambda: xmp.add(h, C, A, B, E, asynchronous=True))
+    h.set_policy(None)
+    got = C.export()
+    want = orc.binary("add", a[perms[1][:S]], b[perms[2][:S]], 8, S)
+    row("add_indexed", ms, 108, E, np.array_equal(got[perms[0][:S]], want))
+    pol.destroy()
     cpu = {}
     t = time.perf_counter()
     orc.binary("add", a, b, 8, E)

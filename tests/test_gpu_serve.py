@@ -155,3 +155,43 @@ def test_errors(handle):
         assert ei.value.name == "xmpErrorInvalidParameter"
     finally:
         srv.destroy()
+
+
+def test_concurrent_submitters(handle):
+    """Submit and Wait from several host threads at once (ctypes releases the GIL in the calls)."""
+    import threading
+    srv = xmp.Server(handle, [1024, 2048], max_slots=2048, max_keys=16, streams=8)
+    try:
+        r1, r2 = _keys(1024, 4, 1000), _keys(2048, 4, 1010)
+        f1, f2 = srv.add_keys(1024, r1), srv.add_keys(2048, r2)
+        per_thread = []
+        for t in range(4):
+            rng = np.random.default_rng(1100 + t)
+            per_thread.append(_requests(rng, [f1, f1 + 1, f1 + 2, f1 + 3], r1, 6, 12, 1200 + 100 * t) +
+                              _requests(rng, [f2, f2 + 1, f2 + 2, f2 + 3], r2, 4, 12, 1250 + 100 * t))
+        results, errors = {}, []
+
+        def worker(t):
+            try:
+                outs = []
+                for k, mm, b, e in per_thread[t]:
+                    o = np.zeros_like(b)
+                    outs.append((srv.submit(k, b, e, o), o))
+                for rid, o in outs:
+                    assert srv.wait(rid, 60_000_000)
+                results[t] = [o for _, o in outs]
+            except Exception as ex:  # reported on the main thread
+                errors.append(ex)
+
+        threads = [threading.Thread(target=worker, args=(t,)) for t in range(4)]
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join(120)
+        assert not errors, errors
+        for t in range(4):
+            for got, want in zip(results[t], _expected(per_thread[t])):
+                assert np.array_equal(got, want)
+        assert srv.stats()["requests_completed"] == sum(len(p) for p in per_thread)
+    finally:
+        srv.destroy()
