@@ -213,6 +213,14 @@ __device__ __forceinline__ void powm_instance(const Group<TPI> &G, const PowmArg
 }
 
 
+// Resident CTAs of 128 threads asked of the register allocator for the
+// persistent kernel: left alone, its extra loop state made the allocator take
+// ~124 registers at 10-12 limbs per lane (4 CTAs/SM) where the one-shot
+// kernel needs 96 (5 CTAs/SM).  The one-shot kernel keeps the allocator's own
+// choice (a bound equal to its natural count still changed its schedule and
+// cost 2.4% at 2048 bits).
+constexpr int powm_batch_min_blocks(int L) { return (L > 8 && L <= 12) ? 5 : 1; }
+
 template <int TPI, int L>
 __global__ void __launch_bounds__(128) powm_kernel(PowmArgs args) {
   Group<TPI> G;
@@ -263,7 +271,7 @@ struct PowmBatchArgs {
 };
 
 template <int TPI, int L>
-__global__ void __launch_bounds__(128) powm_batch_kernel(PowmBatchArgs b) {
+__global__ void __launch_bounds__(128, powm_batch_min_blocks(L)) powm_batch_kernel(PowmBatchArgs b) {
   Group<TPI> G;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   uint32_t *slot = b.table + (size_t)gwarp * ((size_t)32 * L << b.window) + (size_t)(threadIdx.x & 31) * L;
