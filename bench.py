@@ -221,8 +221,17 @@ def run_ours(args, rank, world, local_rank):
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
     lib = xmp.lib()
 
+    forced = None
+    if args.force_config:
+        t, l, w = (int(v) for v in args.force_config.split(","))
+        forced = xmp.PowmConfig(0, t, l, w)
+
     def step():
-        xmp.check(lib.xmpIntegersPowmAsync(h.h, O.x, X.x, E.x, M.x, count), "xmpIntegersPowmAsync")
+        if forced is not None:  # profiling aid: one kernel configuration regardless of the tuner
+            xmp.check(lib.xmpIntegersPowmWithConfigAsync(h.h, O.x, X.x, E.x, M.x, count, ctypes.byref(forced)),
+                      "xmpIntegersPowmWithConfigAsync")
+        else:
+            xmp.check(lib.xmpIntegersPowmAsync(h.h, O.x, X.x, E.x, M.x, count), "xmpIntegersPowmAsync")
 
     for _ in range(args.warmup):
         step()
@@ -715,6 +724,7 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--force-config", default=None, help="lanes,limbs,window: time this powm kernel configuration")
     ap.add_argument("--workload", default="powm2048", choices=["powm2048", "mixed", "serve", "elementwise"])
     ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--serve-peak-requests", type=int, default=3000)
