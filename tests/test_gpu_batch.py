@@ -94,3 +94,27 @@ def test_plan_equals_items_alone(handle):
     plan.destroy()
     for a in arrays:
         a.destroy()
+
+
+def test_plan_argument_errors(handle):
+    """Documented error codes for bad plan arguments; nothing is left allocated."""
+    X, E, M = (handle.integers(512, 8, oracle.random_limbs(40 + k, 8, 16)) for k in range(3))
+    O_bad = handle.integers(1024, 8)   # precision differs from base/mod
+    O_small = handle.integers(512, 4)  # fewer instances than the item's count
+    try:
+        for items, name in (([(O_bad, X, E, M, 8)], "xmpErrorInvalidPrecision"),
+                            ([(O_small, X, E, M, 8)], "xmpErrorInvalidCount")):
+            with pytest.raises(xmp.XmpError) as ei:
+                xmp.BatchPlan(handle, items)
+            assert ei.value.name == name
+        # a CRT item whose output is not twice the half size
+        p = handle.integers(256, 8, oracle.full_length_odd(50, 8, 8))
+        c, out = handle.integers(512, 8), handle.integers(768, 8)
+        with pytest.raises(xmp.XmpError) as ei:
+            xmp.BatchPlan(handle, [], [(out, c, p, p, p, p, p, 8)])
+        assert ei.value.name == "xmpErrorInvalidPrecision"
+        for v in (p, c, out):
+            v.destroy()
+    finally:
+        for v in (X, E, M, O_bad, O_small):
+            v.destroy()

@@ -195,3 +195,25 @@ def test_concurrent_submitters(handle):
         assert srv.stats()["requests_completed"] == sum(len(p) for p in per_thread)
     finally:
         srv.destroy()
+
+
+def test_wait_timeout_and_poll(handle):
+    """Wait with a short timeout (or 0: a poll) reports not-done without retiring the request;
+    a later wait collects the result."""
+    srv = xmp.Server(handle, [4096], max_slots=256, max_keys=32, streams=2)
+    try:
+        m = _keys(4096, 1, 1300)
+        k = srv.add_keys(4096, m)
+        mm = np.repeat(m, 2, axis=0)
+        b = oracle.below(1301, mm)
+        e = oracle.random_limbs(1302, 2, 128)
+        out = np.zeros_like(b)
+        rid = srv.submit(k, b, e, out)
+        assert not srv.wait(rid, 0)        # a 4096-bit exponentiation takes tens of milliseconds
+        assert not srv.wait(rid, 100)      # 0.1 ms is not enough either
+        assert srv.wait(rid, 60_000_000)
+        assert np.array_equal(out, oracle.powm(b, e, mm, 2)[0])
+        with pytest.raises(xmp.XmpError):
+            srv.wait(rid, 0)               # retired once reported done
+    finally:
+        srv.destroy()
