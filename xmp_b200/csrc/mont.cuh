@@ -153,6 +153,24 @@ __device__ __forceinline__ void add_high_halves(uint32_t (&r)[L], uint32_t &c0, 
   c1 = addc_fma(c1);
 }
 
+// Row schedule per shape.  The shuffles of a row -- the next word of b, the
+// quotient digit (lane 0's r[0] once the low halves of a * w are in) and the
+// one-word shift (r[0] once the low halves of n * q are in) -- can be issued
+// as soon as their inputs exist ("early") or where the chains leave them.
+// Which is faster depends on how the scheduler interleaves the chains, so it
+// was measured for every registered shape on a B200 (a full wave of
+// instances and a single instance, 512- and up to 4096-bit exponents) and is
+// fixed here: early where it was faster at a full wave, or where throughput
+// stayed within 1.5% and single-instance latency dropped by 3% or more
+// (e.g. 32 lanes x 3 limbs, 3072 bits: one exponentiation 20.3 -> 16.3 ms;
+// 8 lanes x 4, 1024 bits x 4,096: 3.12 -> 3.01 ms), late elsewhere (e.g.
+// 4 lanes x 12 limbs: 10% slower early).
+__host__ __device__ constexpr bool row_early_shuffles(int TPI, int L) {
+  return (TPI == 2 && (L == 3 || L == 8)) || (TPI == 4 && (L == 1 || L == 3 || L == 5 || L == 6)) ||
+         (TPI == 8 && (L == 3 || L == 4 || L == 5 || L == 6)) || (TPI == 16 && (L == 1 || L == 3 || L == 6)) ||
+         (TPI == 32 && (L == 1 || L == 3 || L == 8 || L == 12));
+}
+
 // r = a * b * R^-1 (mod N), almost reduced (r < R).  a, b < R; r must not alias a or b.
 template <int TPI, int L>
 __device__ __forceinline__ void mont_mul(const Group<TPI> &G, uint32_t (&r)[L], const uint32_t (&a)[L],
@@ -160,26 +178,55 @@ __device__ __forceinline__ void mont_mul(const Group<TPI> &G, uint32_t (&r)[L], 
   uint32_t c0 = 0, c1 = 0;
 #pragma unroll
   for (int k = 0; k < L; k++) r[k] = 0;
+  constexpr bool kEarly = row_early_shuffles(TPI, L);
+  uint32_t w_next = kEarly ? G.bcast(b[0], 0) : 0u;
 #pragma unroll 1
   for (int src = 0; src < TPI; src++) {
 #pragma unroll
     for (int k = 0; k < L; k++) {
-      const uint32_t w = G.bcast(b[k], src);
+      uint32_t w;
+      if constexpr (kEarly) {
+        // the next row's word of b does not depend on this row: broadcast it now
+        w = w_next;
+        w_next = (k + 1 < L) ? G.bcast(b[k + 1 < L ? k + 1 : 0], src) : G.bcast(b[0], src + 1 < TPI ? src + 1 : 0);
+      } else {
+        w = G.bcast(b[k], src);
+      }
       uint64_t p[L], s[L];
       row_products<L>(p, a, w);
-      add_low_halves<L>(r, c0, c1, p);
+      uint32_t q, t;
       // The quotient digit needs only the low word (lane 0's r[0]), final
       // once the low halves of a * w are in; forming the n * q products
       // before the high-half chain of a * w gives the scheduler independent
       // multiplies to overlap with that chain (measured: +3% at 2048 bits).
-      const uint32_t q = G.bcast(r[0], 0) * np0;
-      row_products<L>(s, n, q);
-      add_high_halves<L>(r, c0, c1, p);
-      add_low_halves<L>(r, c0, c1, s);
-      add_high_halves<L>(r, c0, c1, s);
+      if constexpr (kEarly) {
+        r[0] = add_cc(r[0], (uint32_t)p[0]);
+        q = G.bcast(r[0], 0) * np0;
+#pragma unroll
+        for (int j = 1; j < L; j++) r[j] = addc_cc(r[j], (uint32_t)p[j]);
+        c0 = addc_cc(c0, 0u);
+        c1 = addc_fma(c1);
+        row_products<L>(s, n, q);
+        add_high_halves<L>(r, c0, c1, p);
+        // r[0] is final after the first low half of n * q: shift it out now
+        r[0] = add_cc(r[0], (uint32_t)s[0]);
+        t = G.from_next(r[0]);
+#pragma unroll
+        for (int j = 1; j < L; j++) r[j] = addc_cc(r[j], (uint32_t)s[j]);
+        c0 = addc_cc(c0, 0u);
+        c1 = addc_fma(c1);
+        add_high_halves<L>(r, c0, c1, s);
+      } else {
+        add_low_halves<L>(r, c0, c1, p);
+        q = G.bcast(r[0], 0) * np0;
+        row_products<L>(s, n, q);
+        add_high_halves<L>(r, c0, c1, p);
+        add_low_halves<L>(r, c0, c1, s);
+        add_high_halves<L>(r, c0, c1, s);
+        t = G.from_next(r[0]);
+      }
       // divide by 2^32: lane 0's low limb is zero now; every other lane's low
       // limb moves to the top of the lane below, on top of that lane's c0.
-      uint32_t t = G.from_next(r[0]);
 #pragma unroll
       for (int j = 0; j < L - 1; j++) r[j] = r[j + 1];
       r[L - 1] = add_cc(t, c0);
