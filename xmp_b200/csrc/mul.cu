@@ -47,14 +47,21 @@ __device__ __forceinline__ void store_limbs(const uint32_t (&x)[N], const OutVie
   for (uint32_t g = (N + 3) / 4; g < groups; g++) store_group(c.limbs, c.nlimbs, c.stride, e, g, make_uint4(0, 0, 0, 0));
 }
 
-// P = A * B.  Row j adds A * B[j] at word j: the AL products are one
-// mul.wide each (the FMA pipe), folded in by two ALU carry chains -- low
-// halves at j+k, high halves at j+k+1.  The partial product after row j fits
-// in j+AL+1 words, so the chains never carry out of P[j+AL].
 template <int AL, int BL>
-__device__ __forceinline__ void mul_rows(const uint32_t (&A)[AL], const uint32_t (&B)[BL], uint32_t (&P)[AL + BL]) {
+__global__ void __launch_bounds__(256) mul_reg_kernel(ArrayView a, ArrayView b, OutView c, uint32_t count) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  uint32_t ea = in_element(a, i), eb = in_element(b, i), ec = out_element(c, i);
+  if (ec >= c.count) return;
+  uint32_t A[AL], B[BL], P[AL + BL];
+  load_limbs<AL>(A, a, ea);
+  load_limbs<BL>(B, b, eb);
 #pragma unroll
   for (int k = 0; k < AL + BL; k++) P[k] = 0;
+  // Row j adds A * B[j] at word j: the AL products are one mul.wide each (the
+  // FMA pipe), folded in by two ALU carry chains -- low halves at j+k, high
+  // halves at j+k+1.  The partial product after row j fits in j+AL+1 words,
+  // so the chains never carry out of P[j+AL].
 #pragma unroll
   for (int j = 0; j < BL; j++) {
     const uint32_t w = B[j];
@@ -74,131 +81,7 @@ __device__ __forceinline__ void mul_rows(const uint32_t (&A)[AL], const uint32_t
       P[j + AL] += (uint32_t)(p[0] >> 32);
     }
   }
-}
-
-template <int AL, int BL>
-__global__ void __launch_bounds__(256) mul_reg_kernel(ArrayView a, ArrayView b, OutView c, uint32_t count) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  uint32_t ea = in_element(a, i), eb = in_element(b, i), ec = out_element(c, i);
-  if (ec >= c.count) return;
-  uint32_t A[AL], B[BL], P[AL + BL];
-  load_limbs<AL>(A, a, ea);
-  load_limbs<BL>(B, b, eb);
-  mul_rows<AL, BL>(A, B, P);
   store_limbs<AL + BL>(P, c, ec);
-}
-
-// ---- pipelined form for plain (unindexed, unbroadcast) operands ----------
-// A persistent CTA walks tiles of kMulTile consecutive instances.  In the
-// interleaved layout a tile's limb group g of an operand is one contiguous
-// run of kMulTile * 16 bytes, so one thread moves a whole tile into shared
-// memory with a few bulk asynchronous copies (cp.async.bulk, completion
-// counted on an mbarrier) -- the next tile's copies run while the CTA
-// multiplies the current one out of the other stage, keeping HBM busy during
-// the arithmetic.  Waits are bounded: a wait that runs out sets *error and
-// the CTA returns (all its threads together).
-constexpr uint32_t kMulTile = 128;
-
-struct MulPipeArgs {
-  const uint32_t *a;
-  uint32_t a_groups, a_stride;
-  const uint32_t *b;
-  uint32_t b_groups, b_stride;
-  OutView c;
-  uint32_t count;
-  uint32_t *error;
-};
-
-__device__ uint32_t g_mul_pipe_error;
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
-  for (uint32_t spin = 0; spin < (1u << 24); spin++) {
-    uint32_t ok;
-    asm volatile(
-        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (ok) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-               :
-               : "r"(dst), "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
-}
-
-template <int AL, int BL>
-__global__ void __launch_bounds__(kMulTile) mul_pipe_kernel(MulPipeArgs m) {
-  constexpr uint32_t AGM = AL / 4, BGM = BL / 4, SLOTS = AGM + BGM;
-  extern __shared__ uint4 stage[];  // [2][SLOTS][kMulTile]
-  __shared__ __align__(8) uint64_t bars[2];
-  const uint32_t tid = threadIdx.x;
-  const uint32_t ntiles = div_up(m.count, kMulTile);
-  const uint32_t bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
-  if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  auto issue = [&](uint32_t tile, uint32_t s) {
-    const uint32_t base = tile * kMulTile;
-    const uint32_t n = min(kMulTile, m.count - base);
-    uint4 *dst = stage + (size_t)s * SLOTS * kMulTile;
-    const uint32_t bar = s ? bar1 : bar0;
-    // the stage was last read through the generic proxy; order those reads before the async writes
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-                 "r"((m.a_groups + m.b_groups) * n * 16u)
-                 : "memory");
-    for (uint32_t g = 0; g < m.a_groups; g++)
-      bulk_g2s(smem_u32(dst + g * kMulTile), m.a + ((size_t)g * m.a_stride + base) * 4, n * 16u, bar);
-    for (uint32_t g = 0; g < m.b_groups; g++)
-      bulk_g2s(smem_u32(dst + (AGM + g) * kMulTile), m.b + ((size_t)g * m.b_stride + base) * 4, n * 16u, bar);
-  };
-  if (tid == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
-  uint32_t it = 0;
-  for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
-    const uint32_t s = it & 1;
-    const uint32_t next = tile + gridDim.x;
-    if (tid == 0 && next < ntiles) issue(next, s ^ 1);  // freed by the barrier that ended the last iteration
-    const bool ok = mbar_wait_bounded(s ? bar1 : bar0, (it >> 1) & 1);
-    if (!__syncthreads_and(ok)) {
-      if (tid == 0) atomicOr(m.error, 1u);
-      return;
-    }
-    const uint32_t i = tile * kMulTile + tid;
-    if (i < m.count && i < m.c.count) {
-      const uint4 *src = stage + (size_t)s * SLOTS * kMulTile;
-      uint32_t A[AL], B[BL], P[AL + BL];
-#pragma unroll
-      for (uint32_t g = 0; g < AGM; g++) {
-        const uint4 q = g < m.a_groups ? src[g * kMulTile + tid] : make_uint4(0, 0, 0, 0);
-        A[4 * g] = q.x;
-        A[4 * g + 1] = q.y;
-        A[4 * g + 2] = q.z;
-        A[4 * g + 3] = q.w;
-      }
-#pragma unroll
-      for (uint32_t g = 0; g < BGM; g++) {
-        const uint4 q = g < m.b_groups ? src[(AGM + g) * kMulTile + tid] : make_uint4(0, 0, 0, 0);
-        B[4 * g] = q.x;
-        B[4 * g + 1] = q.y;
-        B[4 * g + 2] = q.z;
-        B[4 * g + 3] = q.w;
-      }
-      mul_rows<AL, BL>(A, B, P);
-      store_limbs<AL + BL>(P, m.c, i);
-    }
-    __syncthreads();
-  }
 }
 
 // Column k of the product, accumulated from the interleaved arrays.
@@ -235,32 +118,6 @@ typedef void (*MulLaunch)(ArrayView, ArrayView, OutView, uint32_t, int, cudaStre
 template <int AL, int BL>
 static void launch_mul(ArrayView a, ArrayView b, OutView c, uint32_t count, int threads, cudaStream_t s) {
   mul_reg_kernel<AL, BL><<<grid_for(count, threads), threads, 0, s>>>(a, b, c, count);
-}
-
-typedef void (*MulPipeLaunch)(const MulPipeArgs &, int sm_count, cudaStream_t);
-template <int AL, int BL>
-static void launch_mul_pipe(const MulPipeArgs &m, int sm_count, cudaStream_t s) {
-  static int blocks_per_sm = -1;
-  const size_t smem = (size_t)2 * (AL / 4 + BL / 4) * kMulTile * sizeof(uint4);
-  if (blocks_per_sm < 0) {
-    cudaFuncSetAttribute(mul_pipe_kernel<AL, BL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mul_pipe_kernel<AL, BL>, kMulTile, smem);
-    blocks_per_sm = std::max(occ, 1);
-  }
-  const uint32_t tiles = div_up(m.count, kMulTile);
-  const int grid = (int)std::min<uint64_t>(tiles, (uint64_t)sm_count * blocks_per_sm);
-  mul_pipe_kernel<AL, BL><<<grid, kMulTile, smem, s>>>(m);
-}
-
-#define XMPB_MUL_PIPE_CASE(A, B) \
-  if (al == A && bl == B) return launch_mul_pipe<A, B>;
-static MulPipeLaunch pick_mul_pipe(int al, int bl) {
-  XMPB_MUL_PIPE_CASE(4, 4) XMPB_MUL_PIPE_CASE(8, 4) XMPB_MUL_PIPE_CASE(8, 8) XMPB_MUL_PIPE_CASE(12, 4)
-  XMPB_MUL_PIPE_CASE(12, 8) XMPB_MUL_PIPE_CASE(12, 12) XMPB_MUL_PIPE_CASE(16, 4) XMPB_MUL_PIPE_CASE(16, 8)
-  XMPB_MUL_PIPE_CASE(16, 12) XMPB_MUL_PIPE_CASE(16, 16) XMPB_MUL_PIPE_CASE(24, 8) XMPB_MUL_PIPE_CASE(24, 16)
-  XMPB_MUL_PIPE_CASE(24, 24) XMPB_MUL_PIPE_CASE(32, 16) XMPB_MUL_PIPE_CASE(32, 32)
-  return nullptr;
 }
 
 static const int kClasses[] = {2, 4, 8, 12, 16, 24, 32};
@@ -327,29 +184,10 @@ xmpError_t mul_entry(xmpHandle_t h, xmpIntegers_t p, xmpIntegers_t a, xmpInteger
   xmpError_t e = begin_output(h, p, aliased, indexed || !launch, &t);
   if (e != xmpErrorSuccess) return e;
   OutView vc = view_out(p, t.limbs, pol->indices[0]);
-  // plain operands (no index arrays, no broadcast, no aliasing) stream through the pipelined kernel
-  MulPipeLaunch pipe = nullptr;
-  if (launch && !indexed && !aliased && va.count >= count && vb.count >= count)
-    pipe = pick_mul_pipe(class_of(va.nlimbs), class_of(vb.nlimbs));
-  if (pipe) {
-    MulPipeArgs m;
-    m.a = va.limbs;
-    m.a_groups = div_up(va.nlimbs, 4);
-    m.a_stride = va.stride;
-    m.b = vb.limbs;
-    m.b_groups = div_up(vb.nlimbs, 4);
-    m.b_stride = vb.stride;
-    m.c = vc;
-    m.count = count;
-    void *err = nullptr;
-    if (cudaGetSymbolAddress(&err, g_mul_pipe_error) != cudaSuccess) return xmpErrorCuda;
-    m.error = (uint32_t *)err;
-    pipe(m, (int)h->sm_count, h->stream);
-  } else if (launch) {
+  if (launch)
     launch(va, vb, vc, count, threads, h->stream);
-  } else {
+  else
     mul_stream_kernel<<<grid_for(count, threads), threads, 0, h->stream>>>(va, vb, vc, count);
-  }
   e = end_output(h, p, t);
   if (e != xmpErrorSuccess) return e;
   return check_cuda();
@@ -370,13 +208,6 @@ xmpError_t XMPAPI xmpIntegersMul(xmpHandle_t h, xmpIntegers_t p, const xmpIntege
   if (e != xmpErrorSuccess) return e;
   DeviceGuard guard(h->device);
   cudaStreamSynchronize(h->stream);
-  // a pipelined launch whose copy wait ran out leaves its flag set (never expected: the copies are local)
-  uint32_t flag = 0;
-  if (cudaMemcpyFromSymbol(&flag, g_mul_pipe_error, sizeof(flag)) == cudaSuccess && flag) {
-    const uint32_t zero = 0;
-    cudaMemcpyToSymbol(g_mul_pipe_error, &zero, sizeof(zero));
-    return xmpErrorCuda;
-  }
   return check_cuda();
 }
 
