@@ -150,6 +150,10 @@ xmpError_t XMPAPI xmpSelectorPredict(xmpHandle_t handle, const float *params, co
  * the lookup grid (every 32-bit precision up to 16,384 bits x log2 count x
  * log2 exponent length) and the per-call choice becomes a table lookup. */
 xmpError_t XMPAPI xmpSelectorLoad(xmpHandle_t handle, const float *params);
+/* The same from an ensemble: `members` parameter sets back to back; a cell's
+ * predicted time per slot is the members' mean (independently seeded networks
+ * averaged generalise to untimed precisions better than one). */
+xmpError_t XMPAPI xmpSelectorLoadEnsemble(xmpHandle_t handle, const float *params, int32_t members);
 
 /* ---- serving loop ----------------------------------------------------------
  * No counterpart in the reference.  A server admits modular-exponentiation

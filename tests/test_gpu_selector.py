@@ -3,7 +3,8 @@
 * The CUDA backward pass matches the float64 numpy restatement
   (oracle/selector_ref.py, itself pinned to finite differences on the CPU).
 * CUDA training lowers the loss; CUDA prediction matches the restatement.
-* A loaded selector's grid table drives xmpIntegersPowm choices, and results
+* A loaded selector's grid table (one network, or an ensemble's mean
+  prediction) drives xmpIntegersPowm choices, and results
   stay bit-exact whatever configuration is chosen.
 * With the committed dataset (exhaustive-tuner timings on a B200) and weights,
   the selector's held-out regret is lower than the built-in heuristic's.
@@ -87,9 +88,10 @@ def test_exhaustive_tuner_and_choice_drive_powm(handle):
         v_.destroy()
 
 
-def test_selector_table_lookup(handle):
+@pytest.mark.parametrize("members", [1, 3])
+def test_selector_table_lookup(handle, members):
     shapes, ms = _data(7, n=64)
-    p, _ = tuning.train(handle, shapes, ms, epochs=100, lr=3e-3, seed=1)
+    p, _ = tuning.train_ensemble(handle, shapes, ms, members=members, epochs=100, lr=3e-3, seed=1)
     tuning.install(handle, p)
     try:
         probe = [(2, 2048, 2048, 65536), (2, 1024, 17, 4096), (0, 512, 0, 1 << 18), (1, 1024, 0, 1 << 18)]
@@ -106,7 +108,8 @@ def test_selector_table_lookup(handle):
             eb = int(np.floor(np.log2(max(sh[2], 1))))
             x = np.array([[sh[0] - 1.0, (np.log2(sh[1]) - 10.0) / 4.0, (cb + 0.5 - 13.0) / 7.0,
                            (eb + 0.5 - 7.0) / 7.0 if sh[0] == 2 else -1.0]])
-            pred = ref.forward(p.astype(np.float64), x)[2][0]
+            # an ensemble's table follows the members' mean prediction
+            pred = np.mean([ref.forward(m.astype(np.float64), x)[2][0] for m in tuning.members_of(p)], axis=0)
             masked = np.where(valid, pred, np.inf)
             assert pred[slot.value] <= masked.min() + 1e-3
     finally:

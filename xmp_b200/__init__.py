@@ -98,6 +98,7 @@ _SIGS = {
     "xmpSelectorGradients": [_VP, _VP, _VP, _VP, _I32, _VP, _VP],
     "xmpSelectorPredict": [_VP, _VP, _VP, _I32, _VP],
     "xmpSelectorLoad": [_VP, _VP],
+    "xmpSelectorLoadEnsemble": [_VP, _VP, _I32],
     "xmpPowmBatchPlanCreate": [_VP, _VP, _I32, _VP, _I32, _I32, ctypes.POINTER(_VP)],
     "xmpPowmBatchPlanExecute": [_VP, _VP],
     "xmpPowmBatchPlanDestroy": [_VP, _VP],

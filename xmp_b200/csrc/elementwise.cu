@@ -18,6 +18,7 @@
 // Index arrays: out = indices[0], a = indices[1], b = indices[2] (binary ops);
 // cmp uses indices[0] for a and indices[1] for b; popc uses indices[0].
 #include "internal.h"
+#include <algorithm>
 
 using namespace xmpb;
 
@@ -25,50 +26,59 @@ namespace xmpb {
 
 enum class Bin { Add, Sub, And, Ior, Xor };
 
+// Grid-stride loops over instances: the launch covers at most the GPU's
+// resident threads (stream_grid), so each thread handles several instances
+// instead of the GPU launching and retiring one short-lived CTA per 256.
+#define XMPB_FOR_INSTANCES(i, count)                                                              \
+  for (uint64_t i##_ = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i##_ < (count);            \
+       i##_ += (uint64_t)gridDim.x * blockDim.x)
+
 template <Bin OP>
 __global__ void __launch_bounds__(256) binary_kernel(ArrayView a, ArrayView b, OutView c, uint32_t count) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  uint32_t ea = in_element(a, i), eb = in_element(b, i), ec = out_element(c, i);
-  if (ec >= c.count) return;
-  uint32_t groups = div_up(c.nlimbs, 4);
-  uint32_t carry = (OP == Bin::Sub) ? 1u : 0u;  // subtraction as a + ~b + 1
-  for (uint32_t g = 0; g < groups; g++) {
-    uint4 x = load_group(a.limbs, a.nlimbs, a.stride, ea, g);
-    uint4 y = load_group(b.limbs, b.nlimbs, b.stride, eb, g);
-    uint4 r;
-    if (OP == Bin::Add || OP == Bin::Sub) {
-      if (OP == Bin::Sub) {
-        y.x = ~y.x;
-        y.y = ~y.y;
-        y.z = ~y.z;
-        y.w = ~y.w;
+  XMPB_FOR_INSTANCES(i, count) {
+    const uint32_t i = (uint32_t)i_;
+    uint32_t ea = in_element(a, i), eb = in_element(b, i), ec = out_element(c, i);
+    if (ec >= c.count) continue;
+    uint32_t groups = div_up(c.nlimbs, 4);
+    uint32_t carry = (OP == Bin::Sub) ? 1u : 0u;  // subtraction as a + ~b + 1
+    for (uint32_t g = 0; g < groups; g++) {
+      uint4 x = load_group(a.limbs, a.nlimbs, a.stride, ea, g);
+      uint4 y = load_group(b.limbs, b.nlimbs, b.stride, eb, g);
+      uint4 r;
+      if (OP == Bin::Add || OP == Bin::Sub) {
+        if (OP == Bin::Sub) {
+          y.x = ~y.x;
+          y.y = ~y.y;
+          y.z = ~y.z;
+          y.w = ~y.w;
+        }
+        uint64_t t;
+        t = (uint64_t)x.x + y.x + carry; r.x = (uint32_t)t; carry = (uint32_t)(t >> 32);
+        t = (uint64_t)x.y + y.y + carry; r.y = (uint32_t)t; carry = (uint32_t)(t >> 32);
+        t = (uint64_t)x.z + y.z + carry; r.z = (uint32_t)t; carry = (uint32_t)(t >> 32);
+        t = (uint64_t)x.w + y.w + carry; r.w = (uint32_t)t; carry = (uint32_t)(t >> 32);
+      } else if (OP == Bin::And) {
+        r = make_uint4(x.x & y.x, x.y & y.y, x.z & y.z, x.w & y.w);
+      } else if (OP == Bin::Ior) {
+        r = make_uint4(x.x | y.x, x.y | y.y, x.z | y.z, x.w | y.w);
+      } else {
+        r = make_uint4(x.x ^ y.x, x.y ^ y.y, x.z ^ y.z, x.w ^ y.w);
       }
-      uint64_t t;
-      t = (uint64_t)x.x + y.x + carry; r.x = (uint32_t)t; carry = (uint32_t)(t >> 32);
-      t = (uint64_t)x.y + y.y + carry; r.y = (uint32_t)t; carry = (uint32_t)(t >> 32);
-      t = (uint64_t)x.z + y.z + carry; r.z = (uint32_t)t; carry = (uint32_t)(t >> 32);
-      t = (uint64_t)x.w + y.w + carry; r.w = (uint32_t)t; carry = (uint32_t)(t >> 32);
-    } else if (OP == Bin::And) {
-      r = make_uint4(x.x & y.x, x.y & y.y, x.z & y.z, x.w & y.w);
-    } else if (OP == Bin::Ior) {
-      r = make_uint4(x.x | y.x, x.y | y.y, x.z | y.z, x.w | y.w);
-    } else {
-      r = make_uint4(x.x ^ y.x, x.y ^ y.y, x.z ^ y.z, x.w ^ y.w);
+      store_group(c.limbs, c.nlimbs, c.stride, ec, g, r);
     }
-    store_group(c.limbs, c.nlimbs, c.stride, ec, g, r);
   }
 }
 
 __global__ void __launch_bounds__(256) not_kernel(ArrayView a, OutView c, uint32_t count) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  uint32_t ea = in_element(a, i), ec = out_element(c, i);
-  if (ec >= c.count) return;
-  uint32_t groups = div_up(c.nlimbs, 4);
-  for (uint32_t g = 0; g < groups; g++) {
-    uint4 x = load_group(a.limbs, a.nlimbs, a.stride, ea, g);
-    store_group(c.limbs, c.nlimbs, c.stride, ec, g, make_uint4(~x.x, ~x.y, ~x.z, ~x.w));
+  XMPB_FOR_INSTANCES(i, count) {
+    const uint32_t i = (uint32_t)i_;
+    uint32_t ea = in_element(a, i), ec = out_element(c, i);
+    if (ec >= c.count) continue;
+    uint32_t groups = div_up(c.nlimbs, 4);
+    for (uint32_t g = 0; g < groups; g++) {
+      uint4 x = load_group(a.limbs, a.nlimbs, a.stride, ea, g);
+      store_group(c.limbs, c.nlimbs, c.stride, ec, g, make_uint4(~x.x, ~x.y, ~x.z, ~x.w));
+    }
   }
 }
 
@@ -146,39 +156,46 @@ __global__ void __launch_bounds__(256) shf_smem_kernel(ArrayView a, OutView c, c
 // reference tests the longer operand's extra limbs of instance 0 instead of
 // the selected instance, implementations.h:795; here the selected one.)
 __global__ void __launch_bounds__(256) cmp_kernel(ArrayView a, ArrayView b, int32_t *out, uint32_t count) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  uint32_t ea = in_element(a, i), eb = in_element(b, i);
-  uint32_t groups = div_up(max(a.nlimbs, b.nlimbs), 4);
-  int32_t result = 0;
-  for (int32_t g = (int32_t)groups - 1; g >= 0 && result == 0; g--) {
-    uint4 x = load_group(a.limbs, a.nlimbs, a.stride, ea, g);
-    uint4 y = load_group(b.limbs, b.nlimbs, b.stride, eb, g);
-    if (x.w != y.w) result = x.w > y.w ? 1 : -1;
-    else if (x.z != y.z) result = x.z > y.z ? 1 : -1;
-    else if (x.y != y.y) result = x.y > y.y ? 1 : -1;
-    else if (x.x != y.x) result = x.x > y.x ? 1 : -1;
+  XMPB_FOR_INSTANCES(i, count) {
+    const uint32_t i = (uint32_t)i_;
+    uint32_t ea = in_element(a, i), eb = in_element(b, i);
+    uint32_t groups = div_up(max(a.nlimbs, b.nlimbs), 4);
+    int32_t result = 0;
+    for (int32_t g = (int32_t)groups - 1; g >= 0 && result == 0; g--) {
+      uint4 x = load_group(a.limbs, a.nlimbs, a.stride, ea, g);
+      uint4 y = load_group(b.limbs, b.nlimbs, b.stride, eb, g);
+      if (x.w != y.w) result = x.w > y.w ? 1 : -1;
+      else if (x.z != y.z) result = x.z > y.z ? 1 : -1;
+      else if (x.y != y.y) result = x.y > y.y ? 1 : -1;
+      else if (x.x != y.x) result = x.x > y.x ? 1 : -1;
+    }
+    out[i] = result;
   }
-  out[i] = result;
 }
 
 __global__ void __launch_bounds__(256) popc_kernel(ArrayView a, uint32_t *out, uint32_t count) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  uint32_t ea = in_element(a, i);
-  uint32_t groups = div_up(a.nlimbs, 4), s = 0;
-  uint32_t g = 0;
-  for (; g + 2 <= groups; g += 2) {  // two independent group loads in flight per thread
-    uint4 x = load_group(a.limbs, a.nlimbs, a.stride, ea, g);
-    uint4 y = load_group(a.limbs, a.nlimbs, a.stride, ea, g + 1);
-    s += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w) + __popc(y.x) + __popc(y.y) + __popc(y.z) +
-         __popc(y.w);
+  XMPB_FOR_INSTANCES(i, count) {
+    const uint32_t i = (uint32_t)i_;
+    uint32_t ea = in_element(a, i);
+    uint32_t groups = div_up(a.nlimbs, 4), s = 0;
+    uint32_t g = 0;
+    for (; g + 2 <= groups; g += 2) {  // two independent group loads in flight per thread
+      uint4 x = load_group(a.limbs, a.nlimbs, a.stride, ea, g);
+      uint4 y = load_group(a.limbs, a.nlimbs, a.stride, ea, g + 1);
+      s += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w) + __popc(y.x) + __popc(y.y) + __popc(y.z) +
+           __popc(y.w);
+    }
+    if (g < groups) {
+      uint4 x = load_group(a.limbs, a.nlimbs, a.stride, ea, g);
+      s += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
+    }
+    out[i] = s;
   }
-  if (g < groups) {
-    uint4 x = load_group(a.limbs, a.nlimbs, a.stride, ea, g);
-    s += __popc(x.x) + __popc(x.y) + __popc(x.z) + __popc(x.w);
-  }
-  out[i] = s;
+}
+
+// Grid for the grid-stride kernels: no more CTAs of 256 threads than the GPU holds at once.
+static int stream_grid(xmpHandle_t h, uint32_t count) {
+  return std::min(grid_for(count, 256), (int)h->sm_count * 8);
 }
 
 static bool any_index(xmpExecutionPolicy_t p) {
@@ -201,7 +218,7 @@ static xmpError_t binary_op(xmpHandle_t h, xmpIntegers_t c, xmpIntegers_t a, xmp
   OutTarget t;
   xmpError_t e = begin_output(h, c, c == a || c == b, any_index(p), &t);
   if (e != xmpErrorSuccess) return e;
-  binary_kernel<OP><<<grid_for(count, 256), 256, 0, h->stream>>>(
+  binary_kernel<OP><<<stream_grid(h, count), 256, 0, h->stream>>>(
       view_in(a, p->indices[1], p->indices_count[1]), view_in(b, p->indices[2], p->indices_count[2]),
       view_out(c, t.limbs, p->indices[0]), count);
   e = end_output(h, c, t);
@@ -289,7 +306,7 @@ xmpError_t XMPAPI xmpIntegersNotAsync(xmpHandle_t h, xmpIntegers_t c, const xmpI
   OutTarget t;
   xmpError_t e = begin_output(h, c, c == a, any_index(p), &t);
   if (e != xmpErrorSuccess) return e;
-  not_kernel<<<grid_for(count, 256), 256, 0, h->stream>>>(view_in(a, p->indices[1], p->indices_count[1]),
+  not_kernel<<<stream_grid(h, count), 256, 0, h->stream>>>(view_in(a, p->indices[1], p->indices_count[1]),
                                                            view_out(c, t.limbs, p->indices[0]), count);
   e = end_output(h, c, t);
   if (e != xmpErrorSuccess) return e;
@@ -351,7 +368,7 @@ xmpError_t XMPAPI xmpIntegersCmpAsync(xmpHandle_t h, int32_t *c, const xmpIntege
   ResultBuffer rb;
   xmpError_t e = result_buffer(h, c, (size_t)count * sizeof(int32_t), 0, &rb);
   if (e != xmpErrorSuccess) return e;
-  cmp_kernel<<<grid_for(count, 256), 256, 0, h->stream>>>(view_in(a, p->indices[0], p->indices_count[0]),
+  cmp_kernel<<<stream_grid(h, count), 256, 0, h->stream>>>(view_in(a, p->indices[0], p->indices_count[0]),
                                                            view_in(b, p->indices[1], p->indices_count[1]),
                                                            (int32_t *)rb.dev, count);
   if (rb.host &&
@@ -374,7 +391,7 @@ xmpError_t XMPAPI xmpIntegersPopcAsync(xmpHandle_t h, uint32_t *c, const xmpInte
   ResultBuffer rb;
   xmpError_t e = result_buffer(h, c, (size_t)count * sizeof(uint32_t), 0, &rb);
   if (e != xmpErrorSuccess) return e;
-  popc_kernel<<<grid_for(count, 256), 256, 0, h->stream>>>(view_in(a, p->indices[0], p->indices_count[0]),
+  popc_kernel<<<stream_grid(h, count), 256, 0, h->stream>>>(view_in(a, p->indices[0], p->indices_count[0]),
                                                             (uint32_t *)rb.dev, count);
   if (rb.host &&
       cudaMemcpyAsync(c, rb.dev, (size_t)count * sizeof(uint32_t), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)

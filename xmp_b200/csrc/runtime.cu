@@ -271,8 +271,9 @@ xmpError_t XMPAPI xmpHandleCreateWithMemoryFunctions(xmpHandle_t *handle, xmpAll
   h->sm_count = prop.multiProcessorCount;
   // Configuration choices start from the compiled-in learned selector; if it cannot be
   // loaded (e.g. the caller's allocator refuses), the built-in heuristic stays in charge.
-  if (const float *params = xmpb::default_selector_params()) {
-    if (xmpSelectorLoad(h, params) != xmpErrorSuccess) {
+  int members = 0;
+  if (const float *params = xmpb::default_selector_params(&members)) {
+    if (xmpSelectorLoadEnsemble(h, params, members) != xmpErrorSuccess) {
       xmpTuneClear(h);
       cudaGetLastError();  // a refused allocation is not an error of this call
     }

@@ -91,20 +91,24 @@ __global__ void adam_step(float *p, const float *g, float *m, float *v, int n, f
 
 // One grid cell per thread: forward pass with the weights in shared memory,
 // argmin over the cell's valid slots (valid: bit mask per (op, limbs)).
-__global__ void grid_infer(const float *params, const uint64_t *valid, uint8_t *table) {
+// The table is filled from an ensemble of `members` networks (parameters
+// back to back): a cell's predicted log2(time) per slot is the members'
+// mean, and the cell takes the valid slot with the smallest.  Averaging
+// independently seeded networks generalises to untimed precisions better
+// than any one of them.
+__global__ void grid_infer(const float *params, int members, const uint64_t *valid, uint8_t *table) {
   __shared__ float w[kParams];
-  for (int i = threadIdx.x; i < kParams; i += blockDim.x) w[i] = params[i];
-  __syncthreads();
   const int cells = 3 * kGridMaxLimbs * kGridCountBuckets * kGridExpBuckets;
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= cells) return;
-  int eb = c % kGridExpBuckets, cb = (c / kGridExpBuckets) % kGridCountBuckets;
-  int nl = (c / (kGridExpBuckets * kGridCountBuckets)) % kGridMaxLimbs + 1;
-  int op = c / (kGridExpBuckets * kGridCountBuckets * kGridMaxLimbs);
-  uint64_t vmask = valid[op * kGridMaxLimbs + nl - 1];
-  if (vmask == 0 || (op != xmpTunePowm && eb != 0)) {
-    table[c] = 0xff;
-    return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  int eb = 0, cb = 0, nl = 1, op = 0;
+  uint64_t vmask = 0;
+  if (c < cells) {
+    eb = c % kGridExpBuckets;
+    cb = (c / kGridExpBuckets) % kGridCountBuckets;
+    nl = (c / (kGridExpBuckets * kGridCountBuckets)) % kGridMaxLimbs + 1;
+    op = c / (kGridExpBuckets * kGridCountBuckets * kGridMaxLimbs);
+    vmask = valid[op * kGridMaxLimbs + nl - 1];
+    if (op != xmpTunePowm && eb != 0) vmask = 0;
   }
   // the cell stands for counts in [2^cb, 2^(cb+1)) and exponents in [2^eb, 2^(eb+1)): use the geometric
   // middle.  Batches smaller than the smallest one the tuner times (2^6) leave the GPU just as idle as
@@ -114,25 +118,39 @@ __global__ void grid_infer(const float *params, const uint64_t *valid, uint8_t *
   x[1] = (log2f(32.0f * nl) - 10.0f) / 4.0f;
   x[2] = (fmaxf((float)cb, (float)kSelectorMinCountLog2) + 0.5f - 13.0f) / 7.0f;
   x[3] = op == xmpTunePowm ? ((float)eb + 0.5f - 7.0f) / 7.0f : (0.0f - 7.0f) / 7.0f;
-  float h1[kH], h2[kH];
-  for (int j = 0; j < kH; j++) {
-    float a = w[kOffB1 + j];
-    for (int i = 0; i < kIn; i++) a = fmaf(x[i], w[kOffW1 + i * kH + j], a);
-    h1[j] = fmaxf(a, 0.0f);
+  float acc[kOut];
+  for (int j = 0; j < kOut; j++) acc[j] = 0.0f;
+  // every thread of the block takes part in the loads of every member, cell or not
+  for (int m = 0; m < members; m++) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < kParams; i += blockDim.x) w[i] = params[(size_t)m * kParams + i];
+    __syncthreads();
+    if (vmask == 0) continue;
+    float h1[kH], h2[kH];
+    for (int j = 0; j < kH; j++) {
+      float a = w[kOffB1 + j];
+      for (int i = 0; i < kIn; i++) a = fmaf(x[i], w[kOffW1 + i * kH + j], a);
+      h1[j] = fmaxf(a, 0.0f);
+    }
+    for (int j = 0; j < kH; j++) {
+      float a = w[kOffB2 + j];
+      for (int i = 0; i < kH; i++) a = fmaf(h1[i], w[kOffW2 + i * kH + j], a);
+      h2[j] = fmaxf(a, 0.0f);
+    }
+    for (int j = 0; j < kOut; j++) {
+      if (!((vmask >> j) & 1ull)) continue;
+      float a = w[kOffB3 + j];
+      for (int i = 0; i < kH; i++) a = fmaf(h2[i], w[kOffW3 + i * kOut + j], a);
+      acc[j] += a;
+    }
   }
-  for (int j = 0; j < kH; j++) {
-    float a = w[kOffB2 + j];
-    for (int i = 0; i < kH; i++) a = fmaf(h1[i], w[kOffW2 + i * kH + j], a);
-    h2[j] = fmaxf(a, 0.0f);
-  }
+  if (c >= cells) return;
   int best = 0xff;
   float best_v = 1e30f;
   for (int j = 0; j < kOut; j++) {
     if (!((vmask >> j) & 1ull)) continue;
-    float a = w[kOffB3 + j];
-    for (int i = 0; i < kH; i++) a = fmaf(h2[i], w[kOffW3 + i * kOut + j], a);
-    if (a < best_v) {
-      best_v = a;
+    if (acc[j] < best_v) {
+      best_v = acc[j];
       best = j;
     }
   }
@@ -243,16 +261,18 @@ static void init_params(float *p, uint64_t seed) {
 #include "default_selector.inc"
 #endif
 
-const float *default_selector_params() {
+const float *default_selector_params(int *members) {
 #ifdef XMPB_DEFAULT_SELECTOR_COUNT
-  static_assert(XMPB_DEFAULT_SELECTOR_COUNT == kParams, "embedded selector has the wrong shape");
+  static_assert(XMPB_DEFAULT_SELECTOR_COUNT % kParams == 0, "embedded selector has the wrong shape");
+  *members = XMPB_DEFAULT_SELECTOR_COUNT / kParams;
   return kDefaultSelector;
 #else
+  *members = 0;
   return nullptr;
 #endif
 }
 
-xmpError_t selector_fill_table(xmpHandle_t h, const float *params, std::vector<uint8_t> *table) {
+xmpError_t selector_fill_table(xmpHandle_t h, const float *params, int members, std::vector<uint8_t> *table) {
   const size_t cells = (size_t)3 * kGridMaxLimbs * kGridCountBuckets * kGridExpBuckets;
   std::vector<uint64_t> valid((size_t)3 * kGridMaxLimbs, 0);
   for (int op = 0; op < 3; op++)
@@ -271,16 +291,16 @@ xmpError_t selector_fill_table(xmpHandle_t h, const float *params, std::vector<u
       }
       valid[(size_t)op * kGridMaxLimbs + nl - 1] = mk;
     }
-  float *dp = (float *)h->da(kParams * 4);
+  float *dp = (float *)h->da((size_t)members * kParams * 4);
   uint64_t *dv = (uint64_t *)h->da(valid.size() * 8);
   uint8_t *dt = (uint8_t *)h->da(cells);
   xmpError_t e = xmpErrorSuccess;
   if (!dp || !dv || !dt) {
     e = xmpErrorInvalidCudaMalloc;
   } else {
-    cudaMemcpyAsync(dp, params, kParams * 4, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(dp, params, (size_t)members * kParams * 4, cudaMemcpyHostToDevice, h->stream);
     cudaMemcpyAsync(dv, valid.data(), valid.size() * 8, cudaMemcpyHostToDevice, h->stream);
-    grid_infer<<<grid_for(cells, 128), 128, 0, h->stream>>>(dp, dv, dt);
+    grid_infer<<<grid_for(cells, 128), 128, 0, h->stream>>>(dp, members, dv, dt);
     table->resize(cells);
     cudaMemcpyAsync(table->data(), dt, cells, cudaMemcpyDeviceToHost, h->stream);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) e = xmpErrorCuda;

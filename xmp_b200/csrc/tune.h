@@ -52,9 +52,10 @@ xmpError_t divmod_entry(xmpHandle_t h, xmpIntegers_t q, xmpIntegers_t r, xmpInte
                         uint32_t count, const ElemConfig *forced);
 
 // Selector grid evaluation (selector.cu): fills table[op][limbs-1][cb][eb] with argmin slots.
-xmpError_t selector_fill_table(xmpHandle_t h, const float *params, std::vector<uint8_t> *table);
-// The compiled-in selector parameters (nullptr when the library was built without them).
-const float *default_selector_params();
+xmpError_t selector_fill_table(xmpHandle_t h, const float *params, int members, std::vector<uint8_t> *table);
+// The compiled-in selector: `*members` networks' parameters back to back (nullptr, 0 when the
+// library was built without them).
+const float *default_selector_params(int *members);
 size_t grid_index(int op, uint32_t nlimbs, int count_bucket, int exp_bucket);
 int count_bucket(uint32_t count);
 int exp_bucket(uint32_t exp_bits);

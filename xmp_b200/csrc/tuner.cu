@@ -103,9 +103,18 @@ int tuner_lookup(xmpHandle_t h, int op, uint32_t bits, uint32_t exp_bits, uint32
   return -1;
 }
 
+// An exact tuned choice is taken as it is.  From the selector's table only
+// the kernel (distribution, lanes, limbs) is taken: a window's cost is known
+// exactly -- 2^W - 2 table multiplications plus one per W exponent bits, all
+// with the same kernel -- and the window that minimises it
+// (window_for_bits, up to 7) beats the network's pick, whose fit does not
+// resolve the 1-2% between neighbouring windows.
 bool tuner_lookup_powm(xmpHandle_t h, uint32_t nlimbs, uint32_t exp_bits, uint32_t count, PowmConfig *cfg) {
-  int slot = tuner_lookup(h, xmpTunePowm, nlimbs * 32, exp_bits, count, nullptr);
-  return slot >= 0 && powm_candidate(nlimbs, slot, cfg);
+  int src = 0;
+  int slot = tuner_lookup(h, xmpTunePowm, nlimbs * 32, exp_bits, count, &src);
+  if (slot < 0 || !powm_candidate(nlimbs, slot, cfg)) return false;
+  if (src == 2) cfg->window = window_for_bits(exp_bits);
+  return true;
 }
 
 // ---- synthetic data for the exhaustive tuner ----------------------------------
@@ -299,13 +308,15 @@ xmpError_t XMPAPI xmpTuneClear(xmpHandle_t h) {
   return xmpErrorSuccess;
 }
 
-xmpError_t XMPAPI xmpSelectorLoad(xmpHandle_t h, const float *params) {
-  if (!h || !params) return xmpErrorInvalidParameter;
+xmpError_t XMPAPI xmpSelectorLoadEnsemble(xmpHandle_t h, const float *params, int32_t members) {
+  if (!h || !params || members < 1 || members > 64) return xmpErrorInvalidParameter;
   DeviceGuard guard(h->device);
   TunerState *t = tuner_state(h);
-  xmpError_t e = selector_fill_table(h, params, &t->table);
+  xmpError_t e = selector_fill_table(h, params, members, &t->table);
   t->has_table = (e == xmpErrorSuccess);
   return e;
 }
+
+xmpError_t XMPAPI xmpSelectorLoad(xmpHandle_t h, const float *params) { return xmpSelectorLoadEnsemble(h, params, 1); }
 
 }  // extern "C"

@@ -1,14 +1,16 @@
 """Autotuning and the learned configuration selector (host orchestration).
 
 The tuner and the selector themselves are C/CUDA in libxmp.so
-(include/xmp_b200.h: xmpTuneMeasure, xmpSelectorTrain/Gradients/Predict/Load);
+(include/xmp_b200.h: xmpTuneMeasure, xmpSelectorTrain/Gradients/Predict/Load[Ensemble]);
 this module drives them:
 
   collect  -- time every candidate configuration of every shape of the grid
               (op in {mul, divmod, powm} x bits x batch x powm exponent length)
               on the GPU with the exhaustive tuner; writes a dataset file;
-  train    -- fit the selector MLP with the library's CUDA training kernels on
-              the shapes of 80% of the (op, bits) cells, hold out the rest;
+  train    -- fit an ensemble of independently seeded selector MLPs with the
+              library's CUDA training kernels on the shapes of 80% of the
+              (op, bits) cells, hold out the rest; the members' mean
+              prediction picks the configuration;
   evaluate -- regret t(chosen)/t(best) - 1 of the selector and of the built-in
               heuristic on the held-out shapes, against the exhaustive tuner.
 
@@ -149,12 +151,33 @@ def train(h, shapes, ms, epochs=3000, lr=3e-3, seed=1, params=None):
     return p, loss.value
 
 
-def predict(h, params, shapes):
-    pred = np.zeros((len(shapes), NCAND), dtype=np.float32)
+def train_ensemble(h, shapes, ms, members=5, epochs=3000, lr=3e-3, seed=1):
+    """`members` networks trained from seeds seed, seed+1, ...; parameters back to back."""
+    ps, losses = [], []
+    for k in range(members):
+        p, loss = train(h, shapes, ms, epochs, lr, seed + k)
+        ps.append(p)
+        losses.append(loss)
+    return np.concatenate(ps), losses
+
+
+def members_of(params):
     p = np.ascontiguousarray(params, dtype=np.float32)
-    xmp.check(xmp.lib().xmpSelectorPredict(h.h, p.ctypes.data, shapes_array(shapes), len(shapes), pred.ctypes.data),
-              "xmpSelectorPredict")
-    return pred
+    assert p.size % NPARAMS == 0 and p.size > 0, "selector weights must be a multiple of %d floats" % NPARAMS
+    return p.reshape(-1, NPARAMS)
+
+
+def predict(h, params, shapes):
+    """Predicted log2(ms) per slot; for an ensemble the members' mean (what the grid table uses)."""
+    out = np.zeros((len(shapes), NCAND), dtype=np.float64)
+    mem = members_of(params)
+    for p in mem:
+        pred = np.zeros((len(shapes), NCAND), dtype=np.float32)
+        p = np.ascontiguousarray(p)
+        xmp.check(xmp.lib().xmpSelectorPredict(h.h, p.ctypes.data, shapes_array(shapes), len(shapes),
+                                               pred.ctypes.data), "xmpSelectorPredict")
+        out += pred
+    return (out / len(mem)).astype(np.float32)
 
 
 def gradients(h, params, shapes, ms):
@@ -175,12 +198,42 @@ def choose(pred_row, valid):
     return best
 
 
+_HEURISTIC = {}
+
+
 def heuristic_slot(h, shape):
-    """The built-in heuristic's choice (no tuned entries, no selector)."""
+    """The built-in heuristic's choice (no tuned entries, no selector).  Asked of a
+    handle of its own with the tuner cleared: every new handle starts with the
+    compiled-in selector, whose choice xmpTuneGetChoice would report instead."""
+    hh = _HEURISTIC.get("h")
+    if hh is None:
+        hh = _HEURISTIC["h"] = xmp.Handle()
+        xmp.check(xmp.lib().xmpTuneClear(hh.h), "xmpTuneClear")
     s = ctypes.c_int32(0)
     src = ctypes.c_int32(0)
-    xmp.check(xmp.lib().xmpTuneGetChoice(h.h, ctypes.byref(Shape(*shape)), ctypes.byref(s), ctypes.byref(src)))
+    xmp.check(xmp.lib().xmpTuneGetChoice(hh.h, ctypes.byref(Shape(*shape)), ctypes.byref(s), ctypes.byref(src)))
+    assert src.value == 0
     return s.value
+
+
+def analytic_window(exp_bits, wmax=7):
+    """The window minimising (2^W - 2) + ceil(k / W) multiplications (window_for_bits in the library)."""
+    if exp_bits <= 1:
+        return 1
+    best, cost = 1, None
+    for w in range(1, wmax + 1):
+        c = (1 << w) - 2 + -(-exp_bits // w)
+        if cost is None or c < cost:
+            best, cost = w, c
+    return best
+
+
+def runtime_slot(shape, slot):
+    """The configuration the library runs for a selector choice: for powm the chosen kernel with
+    the analytic window (capped at the six windows the tuner times)."""
+    if shape[0] != OPS["powm"]:
+        return slot
+    return (slot // 6) * 6 + min(analytic_window(shape[2]), 6) - 1
 
 
 def regret_of(ms_row, slot):
@@ -204,7 +257,7 @@ def evaluate(h, params, shapes, ms, idx):
     sel, heu = [], []
     for k, i in enumerate(idx):
         valid = candidate_valid(shapes[i][0], shapes[i][1])
-        sel.append(regret_of(ms[i], choose(pred[k], valid)))
+        sel.append(regret_of(ms[i], runtime_slot(shapes[i], choose(pred[k], valid))))
         heu.append(regret_of(ms[i], heuristic_slot(h, shapes[i])))
     sel, heu = np.array(sel), np.array(heu)
     return {"n": len(idx), "selector_mean_regret": float(sel.mean()) if len(sel) else None,
@@ -221,14 +274,16 @@ def save_weights(path, params):
 
 def load_weights(path=DEFAULT_WEIGHTS):
     p = np.fromfile(path, dtype="<f4")
-    assert p.size == NPARAMS, "selector weights must have %d floats" % NPARAMS
+    members_of(p)
     return p
 
 
 def install(h, params):
-    """Loads a trained selector into the handle (CUDA grid inference -> lookup table)."""
-    p = np.ascontiguousarray(params, dtype=np.float32)
-    xmp.check(xmp.lib().xmpSelectorLoad(h.h, p.ctypes.data), "xmpSelectorLoad")
+    """Loads a trained selector (one network or an ensemble) into the handle (CUDA grid inference ->
+    lookup table)."""
+    mem = members_of(params)
+    p = np.ascontiguousarray(mem.reshape(-1))
+    xmp.check(xmp.lib().xmpSelectorLoadEnsemble(h.h, p.ctypes.data, len(mem)), "xmpSelectorLoadEnsemble")
 
 
 def main():
@@ -246,7 +301,12 @@ def main():
     t.add_argument("--epochs", type=int, default=4000)
     t.add_argument("--lr", type=float, default=3e-3)
     t.add_argument("--seed", type=int, default=1)
+    t.add_argument("--members", type=int, default=5, help="ensemble size (seeds seed .. seed+members-1)")
     t.add_argument("--report", default=None)
+    ev = sub.add_parser("evaluate", help="regret of given weights on a dataset's held-out and training cells")
+    ev.add_argument("--data", default=DEFAULT_DATA)
+    ev.add_argument("--weights", default=DEFAULT_WEIGHTS)
+    ev.add_argument("--report", default=None)
     a = ap.parse_args()
     import torch
     torch.cuda.set_device(0)
@@ -262,12 +322,22 @@ def main():
             shapes = [s for s in shapes if s not in have]
         ms = collect(h, shapes, a.reps, log=lambda s: print(s, flush=True))
         save_dataset(a.out, list(old_shapes) + list(shapes), np.concatenate([old_ms, ms]), meta)
+    elif a.cmd == "evaluate":
+        shapes, ms, meta = load_dataset(a.data)
+        tr, te, held = split_cells(shapes)
+        params = load_weights(a.weights)
+        rep = {"weights": os.path.basename(a.weights), "heldout_cells": [[OP_NAMES[o], b] for o, b in held],
+               "heldout": evaluate(h, params, shapes, ms, te), "train": evaluate(h, params, shapes, ms, tr)}
+        print(json.dumps(rep, indent=1))
+        if a.report:
+            with open(a.report, "w") as f:
+                json.dump(rep, f, indent=1)
     else:
         shapes, ms, meta = load_dataset(a.data)
         tr, te, held = split_cells(shapes)
         t0 = time.time()
-        params, loss = train(h, [shapes[i] for i in tr], ms[tr], a.epochs, a.lr, a.seed)
-        rep = {"train_loss": loss, "train_seconds": time.time() - t0, "train_shapes": len(tr),
+        params, loss = train_ensemble(h, [shapes[i] for i in tr], ms[tr], a.members, a.epochs, a.lr, a.seed)
+        rep = {"members": a.members, "train_loss": loss, "train_seconds": time.time() - t0, "train_shapes": len(tr),
                "heldout_cells": [[OP_NAMES[o], b] for o, b in held],
                "heldout": evaluate(h, params, shapes, ms, te), "train": evaluate(h, params, shapes, ms, tr)}
         save_weights(a.out, params)
