@@ -152,6 +152,65 @@ def test_powm_in_place(handle):
     pol.destroy()
 
 
+def _special_exponents(count, nlimbs, seed):
+    """Exponents that stress a sliding-window scan, interleaved so the instances of one warp
+    follow different schedules: 0, 1, 2, powers of two (trailing zeros), all ones, alternating
+    bits, long zero runs between ones, one-limb and full random values."""
+    e = oracle.random_limbs(seed, count, nlimbs)
+    top = nlimbs * 32 - 1
+    for r in range(count):
+        kind = r % 11
+        v = None
+        if kind == 0:
+            v = 0
+        elif kind == 1:
+            v = 1
+        elif kind == 2:
+            v = 2
+        elif kind == 3:
+            v = 1 << (r * 7 % (top + 1))
+        elif kind == 4:
+            v = (1 << (top + 1)) - 1
+        elif kind == 5:
+            v = int("01" * ((top + 1) // 2), 2)
+        elif kind == 6:
+            v = int("10" * ((top + 1) // 2), 2)
+        elif kind == 7:
+            v = (1 << top) | (1 << (top // 2)) | 1
+        elif kind == 8:
+            v = int(e[r, 0])  # one limb
+        elif kind == 9:
+            v = (1 << top) | (0b1000001 << (r % (top - 8)))
+        if v is not None:
+            e[r] = [(v >> (32 * k)) & 0xFFFFFFFF for k in range(nlimbs)]
+    return e
+
+
+@pytest.mark.parametrize("lanes,limbs", [(2, 8), (4, 5), (8, 4), (16, 2), (1, 8), (8, 1)])
+def test_powm_window_schedules(handle, lanes, limbs):
+    """Every window size 1..7 of a register kernel, with exponents whose schedules differ within a
+    warp.  2 x 8, 4 x 5, 8 x 4 and 16 x 2 run the sliding window (instances that finish early
+    multiply by Mont(1) until the warp is done), 1 x 8 and 8 x 1 the fixed window."""
+    bits = lanes * limbs * 32
+    count = 200
+    m = oracle.full_length_odd(700 + bits, count, bits // 32)
+    x = oracle.below(701 + bits, m)
+    e = _special_exponents(count, bits // 32, 702 + bits)
+    want, _ = oracle.powm(x, e, m, count)
+    X, E, M = (handle.integers(bits, count, v) for v in (x, e, m))
+    O = handle.integers(bits, count)
+    try:
+        for w in range(1, 8):
+            cfg = xmp.PowmConfig(0, lanes, limbs, w)
+            xmp.powm_with_config(handle, O, X, E, M, count, cfg)
+            got = O.export()
+            bad = np.nonzero(~np.all(got == want, axis=1))[0]
+            assert len(bad) == 0, "window %d: mismatch at %s" % (w, bad[:8])
+    finally:
+        for v in (X, E, M, O):
+            v.destroy()
+
+
 def test_powm_every_registered_config(handle):
     """Each (lanes, limbs per lane) kernel at its own capacity, through the default path with a forced config."""
     import ctypes

@@ -268,7 +268,7 @@ xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t h, const xmpPowmBatchItem_t
       if (!tuned)
         c = powm_default_config(b.nlimbs, b.exp_bits, std::max(b.count, kSaturated), xmpAlgorithmDefault,
                                 h->sm_count);
-      c.window = window_for_bits(b.exp_bits);
+      c.window = window_for_bits(b.exp_bits, c.dist != kDistDigit && powm_sliding(c.tpi, c.limbs));
     }
     if (c.dist == kDistDigit) {
       // prefer any register kernel that holds the precision; else digit-serial after the join
@@ -300,10 +300,11 @@ xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t h, const xmpPowmBatchItem_t
     b.blocks = (int)blocks;
     // shrink the window if the tables would exceed the scratch limit
     while (b.cfg.window > 1 &&
-           (size_t)b.blocks * 128 * b.cfg.limbs * ((size_t)4 << b.cfg.window) > scratch_limit(h) / 2)
+           (size_t)b.blocks * 128 * b.cfg.limbs * 4 * powm_table_entries(b.cfg.window, powm_sliding(b.cfg.tpi, b.cfg.limbs)) >
+               scratch_limit(h) / 2)
       b.cfg.window--;
     b.table_offset = bytes;
-    bytes += (size_t)b.blocks * 128 * b.cfg.limbs * ((size_t)4 << b.cfg.window);
+    bytes += (size_t)b.blocks * 128 * b.cfg.limbs * 4 * powm_table_entries(b.cfg.window, powm_sliding(b.cfg.tpi, b.cfg.limbs));
     bytes = (bytes + 255) & ~(size_t)255;
   }
   size_t counter_offset = bytes;

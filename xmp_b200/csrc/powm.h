@@ -55,9 +55,12 @@ struct PowmKernelRegistrar {
                                                   (const void *)powm_batch_kernel<TPI, L>,           \
                                                   powm_launch_r2_##TPI##_##L);
 
-// Best fixed window for a k-bit exponent: minimises table build (2^W - 2
-// multiplies) plus one multiply per window.
-int window_for_bits(uint32_t exp_bits);
+// Window bits for a k-bit exponent.  Sliding window (register kernels with
+// powm_sliding): minimises the table build (2^(W-1) multiplies, weighted 5/4)
+// plus one multiply per window, k/(W+1) on average.  Fixed window (the other
+// register kernels, digit-serial kernel): 2^W - 2 plus k/W.  The two agree at
+// every 32-bit multiple of the standard sizes (128 .. 16,384 bits).
+int window_for_bits(uint32_t exp_bits, bool sliding = true);
 
 // Heuristic configuration for n-limb moduli (used when no tuned entry exists).
 // A nonzero `cap` admits only kernels with exactly cap = lanes x limbs (the

@@ -9,18 +9,34 @@
 //
 // Per instance:
 //   1. N, n0' = -N^-1 mod 2^32, R^2 mod N (exact doublings + Montgomery squarings)
-//   2. window table T[e] = Mont(x^e), e < 2^W: T[0] = R - N, T[1] = Mont(x),
-//      T[e] = T[e-1]*T[1]; stored in the scratch arena, one contiguous slot
-//      of L limbs per lane so every lane moves its limbs with 128-bit accesses
-//   3. left-to-right fixed window over the exponent: W squarings and one table
-//      multiply per window (window value 0 multiplies by T[0], keeping the
-//      control flow independent of the exponent's bits); the next table entry
-//      is loaded before the squarings so its latency is hidden
+//   2. window table, stored in the scratch arena, one contiguous slot of L
+//      limbs per lane so every lane moves its limbs with 128-bit accesses:
+//      slot 0 = R - N (Mont(1)), then for the sliding window the odd powers
+//      Mont(x^(2j-1)), j = 1 .. 2^(W-1) (one squaring for Mont(x^2), then one
+//      multiply per entry), for the fixed window Mont(x^e), e < 2^W
+//   3. the exponent, left to right, by the shape's method (powm_sliding):
+//      sliding window: a zero bit is one squaring; a window of at most W bits
+//      that starts and ends with a one (odd value v, length l) is l squarings
+//      and one multiply by slot (v + 1) / 2.  Every step is one Montgomery
+//      multiply acc * B with B = acc (square) or B = the table entry, chosen
+//      per lane, so the instances of a warp follow their own exponents in one
+//      instruction stream; an instance that has consumed its exponent
+//      multiplies by Mont(1) until the warp's last instance is done.  The
+//      entry is loaded at the multiply step itself (prefetching it into
+//      registers or shared memory a step ahead measured slower: every
+//      squaring's operand select then waited on the load).
+//      fixed window: W squarings and one table multiply per window (value 0
+//      multiplies by Mont(1), keeping the control flow independent of the
+//      exponent's bits); the next entry is loaded before the squarings
 //   4. one Montgomery multiply by 1 and a compare-subtract give x^e mod N
-// The exponent is scanned from the highest window that any instance of the
-// warp needs (warp-uniform, so every shfl sees all 32 lanes); leading zero
-// windows of the reference's full-precision scan (powm_operators.h:55) only
-// square Mont(1) and do not change the result.
+// Against the reference's fixed window (xmp::fwe, powm/powm.h:39-127, 2^W - 2
+// table multiplies and one multiply per W bits) the sliding window takes
+// about 2^(W-1) + k/(W+1) multiplies: ~2,373 instead of 2,450 Montgomery
+// multiplies for a 2048-bit exponent at W = 6 (warp maximum over random
+// exponents).  The sliding scan starts at each instance's own top bit, the
+// fixed one at the warp's highest window; the reference's scan from the full
+// exponent precision (powm_operators.h:55) only squares Mont(1) there, which
+// does not change the result.
 #pragma once
 #include "internal.h"
 #include "mont.cuh"
@@ -35,8 +51,36 @@ struct PowmArgs {
   uint32_t start;   // first op instance of this launch
   uint32_t count;   // op instances in this launch
   uint32_t window;  // window bits W, 1..7
-  uint32_t *table;  // scratch: (launch threads / 32) * 32 * L * 2^W words
+  uint32_t *table;  // scratch: (launch threads / 32) * 32 * L * powm_table_entries(W, powm_sliding(TPI, L)) words
 };
+
+// Exponentiation method of the register kernel with TPI lanes x L limbs:
+// sliding window (true) or fixed window (false).  Per shape, from a B200
+// sweep of every registered kernel with both methods (exponents of
+// min(precision, 2048) bits; a batch of 75,776 / TPI instances and a single
+// instance): the sliding window does ~3-4% fewer Montgomery multiplies but
+// adds per-step control, so it is taken where it is faster at the batch and
+// the batch and single-instance gains together are positive -- the 16-limb
+// shapes and a few mid-size ones (2048 bits, 4 x 16: +0.8%; 3072 bits,
+// 16 x 6: +4.8%; 1280 bits, 8 x 5: +8.1%).  It loses at 12 limbs per lane
+// (-7 to -9%: the compiler's schedule of the multiply inside the sliding loop
+// is worse there) and at small precisions, where the control is a larger
+// share of a step.
+__host__ __device__ constexpr bool powm_sliding(int TPI, int L) {
+  return (TPI == 1 && (L == 24 || L == 32)) ||
+         (TPI == 2 && (L == 8 || L == 16)) ||
+         (TPI == 4 && (L == 5 || L == 6 || L == 16)) ||
+         (TPI == 8 && (L == 4 || L == 5 || L == 6 || L == 16)) ||
+         (TPI == 16 && (L == 2 || L == 4 || L == 6 || L == 16)) ||
+         (TPI == 32 && (L == 8 || L == 16));
+}
+
+// Window-table entries for window bits W.  Sliding: slot 0 holds Mont(1) and
+// slot j >= 1 Mont(x^(2j-1)), the odd powers a sliding window multiplies by.
+// Fixed: slot e holds Mont(x^e), e < 2^W.
+__host__ __device__ constexpr uint32_t powm_table_entries(uint32_t W, bool sliding) {
+  return sliding ? (W ? (1u << (W - 1)) + 1u : 1u) : (1u << W);
+}
 
 template <int TPI, int L>
 __device__ __forceinline__ void load_lane_limbs(uint32_t (&x)[L], const uint32_t *limbs, uint32_t nlimbs,
@@ -121,6 +165,68 @@ __device__ __forceinline__ uint32_t exp_window(const ArrayView &ex, uint32_t e, 
   return v & ((1u << w) - 1u);
 }
 
+// Sliding-window scan over one exponent element.  `pos` is the highest bit
+// not yet consumed; `cur` holds word pos / 32 and `nxt` the word below it,
+// loaded one word ahead, so a scan waits for memory only after a whole zero
+// word.
+struct ExpCursor {
+  int32_t pos;
+  uint32_t cur, nxt;
+};
+
+__device__ __forceinline__ void cursor_init(ExpCursor &c, const ArrayView &ex, uint32_t e, int32_t pos) {
+  c.pos = pos;
+  c.cur = c.nxt = 0;
+  if (pos >= 0) {
+    const uint32_t j = (uint32_t)pos >> 5;
+    c.cur = load_limb(ex.limbs, ex.nlimbs, ex.stride, e, j);
+    if (j) c.nxt = load_limb(ex.limbs, ex.nlimbs, ex.stride, e, j - 1);
+  }
+}
+
+// Steps down to word j (the current `nxt`) and loads the word below it.
+__device__ __forceinline__ void cursor_down(ExpCursor &c, const ArrayView &ex, uint32_t e, uint32_t j) {
+  c.cur = c.nxt;
+  c.nxt = j ? load_limb(ex.limbs, ex.nlimbs, ex.stride, e, j - 1) : 0u;
+}
+
+// Skips zero bits and takes the next window of at most W bits that starts and
+// ends with a one: *sq = the squarings before its multiply (skipped zeros +
+// window length), *idx = its table slot ((v + 1) / 2 for the odd window value
+// v).  Returns false when no one bit is left (*sq = the trailing zero bits).
+__device__ __forceinline__ bool next_window(const ArrayView &ex, uint32_t e, ExpCursor &c, uint32_t W, uint32_t *sq,
+                                            uint32_t *idx) {
+  uint32_t zeros = 0;
+  while (c.pos >= 0) {
+    const uint32_t j = (uint32_t)c.pos >> 5, b = (uint32_t)c.pos & 31;
+    const uint32_t w = c.cur & ((2u << b) - 1u);  // bits <= pos of this word
+    if (w == 0) {
+      zeros += b + 1;
+      c.pos = (int32_t)(j * 32) - 1;
+      if (j) cursor_down(c, ex, e, j - 1);
+      continue;
+    }
+    const uint32_t tb = 31 - __clz(w);  // the window's top bit, within the word
+    zeros += b - tb;
+    const int32_t top = (int32_t)(j * 32 + tb);
+    uint32_t l = min(W, (uint32_t)top + 1);
+    // bits [top - l + 1, top]; a window reaching below bit 0 of the word continues in nxt (j >= 1 then)
+    uint32_t v = tb + 1 >= l ? c.cur >> (tb + 1 - l) : (c.cur << (l - tb - 1)) | (c.nxt >> (33 - l + tb));
+    v &= (1u << l) - 1u;  // top bit set: v != 0
+    const uint32_t tz = __ffs(v) - 1;
+    v >>= tz;
+    l -= tz;
+    c.pos = top - (int32_t)l;
+    if (c.pos >= 0 && ((uint32_t)c.pos >> 5) != j) cursor_down(c, ex, e, j - 1);
+    *sq = zeros + l;
+    *idx = (v + 1) >> 1;
+    return true;
+  }
+  *sq = zeros;
+  *idx = 0;
+  return false;
+}
+
 // Bit length of the exponent element, scanned by the group's lanes in parallel.
 template <int TPI>
 __device__ __forceinline__ uint32_t exp_bitlen(const Group<TPI> &G, const ArrayView &ex, uint32_t e) {
@@ -148,14 +254,23 @@ __device__ __forceinline__ void powm_instance(const Group<TPI> &G, const PowmArg
   const uint32_t np0 = neg_inv32(G.bcast(n[0], 0));
 
   const uint32_t W = args.window;
-  uint32_t ebits = exp_bitlen<TPI>(G, args.exp, ee);
-  ebits = __reduce_max_sync(kFull, ebits);
-  const uint32_t nwin = ebits ? (ebits + W - 1) / W : 1;
+  constexpr bool kSliding = powm_sliding(TPI, L);
+  // sliding: from this instance's own top bit (its lanes agree), instances of a warp scan independently;
+  // fixed: from the highest window any instance of the warp needs (warp-uniform)
+  ExpCursor cur;
+  uint32_t nwin = 0;
+  if constexpr (kSliding) {
+    cursor_init(cur, args.exp, ee, (int32_t)exp_bitlen<TPI>(G, args.exp, ee) - 1);
+  } else {
+    uint32_t ebits = exp_bitlen<TPI>(G, args.exp, ee);
+    ebits = __reduce_max_sync(kFull, ebits);
+    nwin = ebits ? (ebits + W - 1) / W : 1;
+  }
 
   const size_t entry_stride = (size_t)32 * L;
 
   uint32_t x[L], t[L], acc[L];
-  // T[0] = R - N, a representative of Mont(1) below R
+  // slot 0 = R - N, a representative of Mont(1) below R
 #pragma unroll
   for (int k = 0; k < L; k++) acc[k] = 0;
   dsub<TPI, L>(G, acc, n, kFull);
@@ -167,36 +282,88 @@ __device__ __forceinline__ void powm_instance(const Group<TPI> &G, const PowmArg
     else
       compute_r2<TPI, L>(G, r2, n, np0);
     load_lane_limbs<TPI, L>(x, args.base.limbs, args.base.nlimbs, args.base.stride, eb, G.lane);
-    mont_mul<TPI, L>(G, t, x, r2, n, np0);  // T[1] = Mont(x)
+    mont_mul<TPI, L>(G, t, x, r2, n, np0);  // slot 1 = Mont(x)
   }
   slot_store<L>(slot + entry_stride, t);
-#pragma unroll
-  for (int k = 0; k < L; k++) acc[k] = t[k];
-  const uint32_t entries = 1u << W;
-#pragma unroll 1
-  for (uint32_t e = 2; e < entries; e++) {
-    mont_mul<TPI, L>(G, x, acc, t, n, np0);
-#pragma unroll
-    for (int k = 0; k < L; k++) acc[k] = x[k];
-    slot_store<L>(slot + e * entry_stride, acc);
-  }
 
-  // Main loop: acc holds the running power in Montgomery form.
-  uint32_t win = exp_window(args.exp, ee, (nwin - 1) * W, W);
-  slot_load<L>(slot + win * entry_stride, acc);
-#pragma unroll 1
-  for (int32_t wi = (int32_t)nwin - 2; wi >= 0; wi--) {
-    win = exp_window(args.exp, ee, (uint32_t)wi * W, W);
-    uint32_t y[L];
-    slot_load<L>(slot + win * entry_stride, y);
-#pragma unroll 1
-    for (uint32_t s = 0; s <= W; s++) {
-      uint32_t bsel[L];
+  if constexpr (kSliding) {
+    // slots 2 .. 2^(W-1): Mont(x^3), Mont(x^5), ...
+    const uint32_t half = 1u << (W - 1);
+    if (half > 1) {
+      mont_mul<TPI, L>(G, x, t, t, n, np0);  // Mont(x^2)
 #pragma unroll
-      for (int k = 0; k < L; k++) bsel[k] = (s < W) ? acc[k] : y[k];
+      for (int k = 0; k < L; k++) {
+        acc[k] = t[k];
+        t[k] = x[k];
+      }
+#pragma unroll 1
+      for (uint32_t j = 2; j <= half; j++) {
+        mont_mul<TPI, L>(G, x, acc, t, n, np0);
+#pragma unroll
+        for (int k = 0; k < L; k++) acc[k] = x[k];
+        slot_store<L>(slot + j * entry_stride, acc);
+      }
+    }
+
+    // The first window sets acc (Mont(1) for a zero exponent); then each step is
+    // one multiply acc * B: B = acc before step mul_at and, from it on, table
+    // slot yidx (the next window's entry, or Mont(1) once the exponent is
+    // consumed), loaded at the multiply itself -- other warps cover its latency,
+    // and nothing waits on it in the squarings.
+    uint32_t sq, yidx;
+    next_window(args.exp, ee, cur, W, &sq, &yidx);
+    slot_load<L>(slot + yidx * entry_stride, acc);
+    bool more = next_window(args.exp, ee, cur, W, &sq, &yidx);
+    uint32_t mul_at = sq;
+#pragma unroll 1
+    for (uint32_t step = 0; __any_sync(kFull, more || step < mul_at); step++) {
+      const bool use_y = step >= mul_at;
+      uint32_t bsel[L];
+      if (use_y) {
+        slot_load<L>(slot + yidx * entry_stride, bsel);
+      } else {
+#pragma unroll
+        for (int k = 0; k < L; k++) bsel[k] = acc[k];
+      }
       mont_mul<TPI, L>(G, x, acc, bsel, n, np0);
 #pragma unroll
       for (int k = 0; k < L; k++) acc[k] = x[k];
+      if (use_y && more) {
+        more = next_window(args.exp, ee, cur, W, &sq, &yidx);
+        mul_at = step + 1 + sq;
+      }
+    }
+  } else {
+    // slots 2 .. 2^W - 1: Mont(x^e)
+#pragma unroll
+    for (int k = 0; k < L; k++) acc[k] = t[k];
+    const uint32_t entries = 1u << W;
+#pragma unroll 1
+    for (uint32_t e = 2; e < entries; e++) {
+      mont_mul<TPI, L>(G, x, acc, t, n, np0);
+#pragma unroll
+      for (int k = 0; k < L; k++) acc[k] = x[k];
+      slot_store<L>(slot + e * entry_stride, acc);
+    }
+
+    // W squarings and one table multiply per window (window value 0 multiplies
+    // by Mont(1)); the window's entry is loaded before its squarings.
+    uint32_t win = exp_window(args.exp, ee, (nwin - 1) * W, W);
+    slot_load<L>(slot + win * entry_stride, acc);
+#pragma unroll 1
+    for (int32_t wi = (int32_t)nwin - 2; wi >= 0; wi--) {
+      win = exp_window(args.exp, ee, (uint32_t)wi * W, W);
+      uint32_t y[L];
+      slot_load<L>(slot + win * entry_stride, y);
+#pragma unroll 1
+      for (uint32_t s = 0; s <= W; s++) {
+        uint32_t bsel[L];
+#pragma unroll
+        for (int k = 0; k < L; k++) bsel[k] = (s < W) ? acc[k] : y[k];
+        mont_mul<TPI, L>(G, x, acc, bsel, n, np0);
+#pragma unroll
+        for (int k = 0; k < L; k++) acc[k] = x[k];
+      }
     }
   }
 
@@ -229,7 +396,8 @@ __global__ void __launch_bounds__(128) powm_kernel(PowmArgs args) {
   const bool valid = local < args.count;
   // Lanes past the end run a copy of the last instance so every shfl sees a full warp.
   const uint32_t i = args.start + (valid ? local : args.count - 1);
-  uint32_t *slot = args.table + (size_t)(gtid >> 5) * ((size_t)32 * L << args.window) + (size_t)(threadIdx.x & 31) * L;
+  uint32_t *slot = args.table + (size_t)(gtid >> 5) * ((size_t)32 * L * powm_table_entries(args.window, powm_sliding(TPI, L))) +
+                   (size_t)(threadIdx.x & 31) * L;
   powm_instance<TPI, L>(G, args, i, valid, slot);
 }
 
@@ -274,7 +442,8 @@ template <int TPI, int L>
 __global__ void __launch_bounds__(128, powm_batch_min_blocks(L)) powm_batch_kernel(PowmBatchArgs b) {
   Group<TPI> G;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  uint32_t *slot = b.table + (size_t)gwarp * ((size_t)32 * L << b.window) + (size_t)(threadIdx.x & 31) * L;
+  uint32_t *slot = b.table + (size_t)gwarp * ((size_t)32 * L * powm_table_entries(b.window, powm_sliding(TPI, L))) +
+                   (size_t)(threadIdx.x & 31) * L;
   constexpr uint32_t per_item = 32 / TPI;
   while (true) {
     uint32_t item = 0;

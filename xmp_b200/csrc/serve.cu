@@ -215,7 +215,7 @@ static void choose_configs(xmpServer_t s, Class &c) {
               (uint32_t)(cfg.tpi * cfg.limbs) == c.cap && powm_find(cfg.tpi, cfg.limbs);
     if (!ok) {
       cfg = powm_default_config(c.n, c.precision, ops, xmpAlgorithmDefault, s->h->sm_count, c.cap);
-      cfg.window = window_for_bits(c.precision);
+      cfg.window = window_for_bits(c.precision, powm_sliding(cfg.tpi, cfg.limbs));
     }
     c.cfg[b] = cfg;
     c.entry[b] = powm_find(cfg.tpi, cfg.limbs);
@@ -517,7 +517,7 @@ xmpError_t XMPAPI xmpServerCreate(xmpHandle_t h, const uint32_t *precisions, uin
     size_t tw = 0;
     for (int b = 0; b < kBuckets; b++) {
       if (!c.entry[b]) return fail(xmpErrorUnsupported);
-      tw = std::max(tw, (size_t)cap << c.cfg[b].window);
+      tw = std::max(tw, (size_t)cap * powm_table_entries(c.cfg[b].window, powm_sliding(c.cfg[b].tpi, c.cfg[b].limbs)));
     }
     c.table_words = tw;
     c.kcap = round_up(cf.max_keys, 32);

@@ -113,7 +113,7 @@ bool tuner_lookup_powm(xmpHandle_t h, uint32_t nlimbs, uint32_t exp_bits, uint32
   int src = 0;
   int slot = tuner_lookup(h, xmpTunePowm, nlimbs * 32, exp_bits, count, &src);
   if (slot < 0 || !powm_candidate(nlimbs, slot, cfg)) return false;
-  if (src == 2) cfg->window = window_for_bits(exp_bits);
+  if (src == 2) cfg->window = window_for_bits(exp_bits, cfg->dist != kDistDigit && powm_sliding(cfg->tpi, cfg->limbs));
   return true;
 }
 

@@ -216,13 +216,15 @@ def heuristic_slot(h, shape):
     return s.value
 
 
-def analytic_window(exp_bits, wmax=7):
-    """The window minimising (2^W - 2) + ceil(k / W) multiplications (window_for_bits in the library)."""
+def analytic_window(exp_bits, wmax=7, sliding=True):
+    """window_for_bits in the library: the window minimising the table build plus one multiply per
+    window -- 1.25 * 2^(W-1) + ceil(k / (W+1)) for the register kernels' sliding window, (2^W - 2) +
+    ceil(k / W) for the digit-serial kernel's fixed window."""
     if exp_bits <= 1:
         return 1
     best, cost = 1, None
     for w in range(1, wmax + 1):
-        c = (1 << w) - 2 + -(-exp_bits // w)
+        c = 1.25 * (1 << (w - 1)) + -(-exp_bits // (w + 1)) if sliding else (1 << w) - 2 + -(-exp_bits // w)
         if cost is None or c < cost:
             best, cost = w, c
     return best
@@ -230,10 +232,13 @@ def analytic_window(exp_bits, wmax=7):
 
 def runtime_slot(shape, slot):
     """The configuration the library runs for a selector choice: for powm the chosen kernel with
-    the analytic window (capped at the six windows the tuner times)."""
+    the analytic window (capped at the six windows the tuner times).  Register kernels take the
+    sliding-window rule here; the fixed-window kernels' rule gives the same window at every
+    exponent length of the dataset (17, 256, 1024 and the full precisions)."""
     if shape[0] != OPS["powm"]:
         return slot
-    return (slot // 6) * 6 + min(analytic_window(shape[2]), 6) - 1
+    d = slot // 6
+    return d * 6 + min(analytic_window(shape[2], sliding=d < 6), 6) - 1
 
 
 def regret_of(ms_row, slot):
