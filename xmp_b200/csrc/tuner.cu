@@ -239,12 +239,20 @@ xmpError_t XMPAPI xmpTuneMeasure(xmpHandle_t h, const xmpTuneShape_t *shape, int
     float t = 1e30f;
     int runs = std::max(1, (int)reps);
     for (int r = 0; r < runs + 1 && e == xmpErrorSuccess; r++) {
+      const size_t arenas = h->scratch_size + h->tmp_out_size;
       cudaEventRecord(t0, h->stream);
       e = run();
       cudaEventRecord(t1, h->stream);
       cudaEventSynchronize(t1);
       float f = 0;
       cudaEventElapsedTime(&f, t0, t1);
+      // A run that grew the scratch or output arena timed its cudaMalloc (the
+      // device idles between the events while the host allocates): not a
+      // timing of the kernel, so it is run again.
+      if (h->scratch_size + h->tmp_out_size != arenas) {
+        r--;
+        continue;
+      }
       if (r > 0 || runs == 1) t = std::min(t, f);
       // A candidate far slower than the best so far is not repeated, and the
       // other windows of its distribution are not timed at all.
