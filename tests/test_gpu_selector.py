@@ -7,7 +7,8 @@
   prediction) drives xmpIntegersPowm choices, and results
   stay bit-exact whatever configuration is chosen.
 * With the committed dataset (exhaustive-tuner timings on a B200) and weights,
-  the selector's held-out regret is lower than the built-in heuristic's.
+  the selector's regret on the held-out shapes is lower than the built-in
+  heuristic's and within 5%.
 """
 import ctypes
 import os
@@ -119,8 +120,12 @@ def test_selector_table_lookup(handle, members):
 @pytest.mark.skipif(not (os.path.exists(tuning.DEFAULT_DATA) and os.path.exists(tuning.DEFAULT_WEIGHTS)),
                     reason="no committed tuning dataset / selector weights")
 def test_committed_selector_beats_heuristic(handle):
+    """The compiled-in selector was trained on 80% of the measured shapes; on the other 20% (batch
+    sizes and exponent lengths it has not seen, at the measured precisions) its choices cost less
+    than the built-in heuristic's, and stay within the 5% regret target."""
     shapes, ms, _ = tuning.load_dataset(tuning.DEFAULT_DATA)
     params = tuning.load_weights()
-    tr, te, held = tuning.split_cells(shapes)
+    tr, te = tuning.splits(shapes)["shapes"]
     r = tuning.evaluate(handle, params, shapes, ms, te)
     assert r["selector_mean_regret"] <= r["heuristic_mean_regret"] + 1e-9, r
+    assert r["selector_mean_regret"] <= 0.05, r

@@ -35,6 +35,12 @@ def test_grid_and_regret_bookkeeping():
     cells = {(s[0], s[1]) for s in g}
     assert 0.15 <= len(held) / len(cells) <= 0.25
     assert not ({(g[i][0], g[i][1]) for i in tr} & set(held))
+    # held-out shapes within the measured precisions: disjoint, complete, ~20%, deterministic
+    tr2, te2 = tuning.split_shapes(g)
+    assert not (set(tr2) & set(te2)) and sorted(tr2 + te2) == list(range(len(g)))
+    assert 0.18 <= len(te2) / len(g) <= 0.22
+    assert (tr2, te2) == tuning.split_shapes(g)
+    assert set(tuning.splits(g)) == {"cells", "shapes"}
     row = np.full(48, -1.0, dtype=np.float32)
     row[[0, 1, 6]] = [2.0, 1.0, 4.0]
     row[7] = np.nan

@@ -8,11 +8,13 @@ this module drives them:
               (op in {mul, divmod, powm} x bits x batch x powm exponent length)
               on the GPU with the exhaustive tuner; writes a dataset file;
   train    -- fit an ensemble of independently seeded selector MLPs with the
-              library's CUDA training kernels on the shapes of 80% of the
-              (op, bits) cells, hold out the rest; the members' mean
-              prediction picks the configuration;
+              library's CUDA training kernels on 80% of the shapes (--split
+              shapes, the shipped selector) or on the shapes of 80% of the
+              (op, bits) cells (--split cells); the members' mean prediction
+              picks the configuration;
   evaluate -- regret t(chosen)/t(best) - 1 of the selector and of the built-in
-              heuristic on the held-out shapes, against the exhaustive tuner.
+              heuristic against the exhaustive tuner, on both held-out sets:
+              shapes within the measured precisions, and whole precisions.
 
   python -m xmp_b200.tuning collect --out xmp_b200/tuning/b200_dataset.json
   python -m xmp_b200.tuning train --data xmp_b200/tuning/b200_dataset.json --out xmp_b200/tuning/b200_selector.f32
@@ -138,6 +140,27 @@ def split_cells(shapes, holdout=0.2, seed=7):
     train = [i for i, s in enumerate(shapes) if (s[0], s[1]) not in held]
     test = [i for i, s in enumerate(shapes) if (s[0], s[1]) in held]
     return train, test, sorted(held)
+
+
+def split_shapes(shapes, holdout=0.2, seed=7):
+    """80/20 split by shape within the measured precisions: every (op, bits) cell keeps most of its
+    shapes for training and holds out the others (other batch sizes and exponent lengths at the
+    same precision).  The held-out list is the selector's use within the precisions it was
+    measured on; `split_cells` holds out whole precisions instead (extrapolation)."""
+    rnd = random.Random(seed)
+    idx = list(range(len(shapes)))
+    rnd.shuffle(idx)
+    k = max(1, int(round(len(shapes) * holdout)))
+    held = set(idx[:k])
+    return [i for i in range(len(shapes)) if i not in held], sorted(held)
+
+
+def splits(shapes):
+    """(train, heldout) indices of both evaluations: 'cells' (whole held-out precisions) and
+    'shapes' (held-out shapes within the measured precisions)."""
+    tr_c, te_c, _ = split_cells(shapes)
+    tr_s, te_s = split_shapes(shapes)
+    return {"cells": (tr_c, te_c), "shapes": (tr_s, te_s)}
 
 
 def train(h, shapes, ms, epochs=3000, lr=3e-3, seed=1, params=None):
@@ -308,6 +331,8 @@ def main():
     t.add_argument("--seed", type=int, default=1)
     t.add_argument("--members", type=int, default=5, help="ensemble size (seeds seed .. seed+members-1)")
     t.add_argument("--report", default=None)
+    t.add_argument("--split", default="shapes", choices=["shapes", "cells"],
+                   help="training shapes: all but the held-out shapes (default) or all but the held-out cells")
     ev = sub.add_parser("evaluate", help="regret of given weights on a dataset's held-out and training cells")
     ev.add_argument("--data", default=DEFAULT_DATA)
     ev.add_argument("--weights", default=DEFAULT_WEIGHTS)
@@ -329,22 +354,26 @@ def main():
         save_dataset(a.out, list(old_shapes) + list(shapes), np.concatenate([old_ms, ms]), meta)
     elif a.cmd == "evaluate":
         shapes, ms, meta = load_dataset(a.data)
-        tr, te, held = split_cells(shapes)
         params = load_weights(a.weights)
-        rep = {"weights": os.path.basename(a.weights), "heldout_cells": [[OP_NAMES[o], b] for o, b in held],
-               "heldout": evaluate(h, params, shapes, ms, te), "train": evaluate(h, params, shapes, ms, tr)}
+        _, _, held = split_cells(shapes)
+        rep = {"weights": os.path.basename(a.weights), "heldout_cells": [[OP_NAMES[o], b] for o, b in held]}
+        for name, (tr, te) in splits(shapes).items():
+            rep[name] = {"heldout": evaluate(h, params, shapes, ms, te), "train": evaluate(h, params, shapes, ms, tr)}
         print(json.dumps(rep, indent=1))
         if a.report:
             with open(a.report, "w") as f:
                 json.dump(rep, f, indent=1)
     else:
         shapes, ms, meta = load_dataset(a.data)
-        tr, te, held = split_cells(shapes)
+        tr, te = splits(shapes)[a.split]
+        _, _, held = split_cells(shapes)
         t0 = time.time()
         params, loss = train_ensemble(h, [shapes[i] for i in tr], ms[tr], a.members, a.epochs, a.lr, a.seed)
-        rep = {"members": a.members, "train_loss": loss, "train_seconds": time.time() - t0, "train_shapes": len(tr),
-               "heldout_cells": [[OP_NAMES[o], b] for o, b in held],
-               "heldout": evaluate(h, params, shapes, ms, te), "train": evaluate(h, params, shapes, ms, tr)}
+        rep = {"members": a.members, "split": a.split, "train_loss": loss, "train_seconds": time.time() - t0,
+               "train_shapes": len(tr), "heldout": evaluate(h, params, shapes, ms, te),
+               "train": evaluate(h, params, shapes, ms, tr)}
+        if a.split == "cells":
+            rep["heldout_cells"] = [[OP_NAMES[o], b] for o, b in held]
         save_weights(a.out, params)
         print(json.dumps(rep, indent=1))
         if a.report:
