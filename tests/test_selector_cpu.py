@@ -47,3 +47,15 @@ def test_grid_and_regret_bookkeeping():
     assert tuning.regret_of(row, 1) == 0.0
     assert abs(tuning.regret_of(row, 0) - 1.0) < 1e-9
     assert tuning.regret_of(row, 7) >= 3.0  # untimed window of a slow distribution
+
+
+def test_window_rules_agree_on_dataset_exponents():
+    """The evaluation maps a selector slot to the window the library would run with the
+    sliding-window rule; the fixed-window kernels' rule must give the same window at every
+    exponent length the dataset holds, or that mapping would be inexact for them."""
+    from xmp_b200 import tuning
+    lengths = {s[2] for s in tuning.grid(150.0) if s[0] == tuning.OPS["powm"]}
+    assert lengths
+    for k in sorted(lengths):
+        assert tuning.analytic_window(k, sliding=True) == tuning.analytic_window(k, sliding=False), k
+
