@@ -617,7 +617,8 @@ xmpError_t XMPAPI xmpServerAddKeys(xmpServer_t s, uint32_t precision, const uint
   xmpError_t e = xmpErrorSuccess;
   if (cudaMemcpyAsync(rows, moduli, bytes, cudaMemcpyHostToDevice, s->setup) != cudaSuccess) e = xmpErrorCuda;
   if (!e) {
-    rows_to_slots<<<dim3(div_up(count, 128), c.ngroups, 1), 128, 0, s->setup>>>(rows, c.key_mod, rows, c.key_mod,
+    // one pair (grid.z = 1): the second pair is never read
+    rows_to_slots<<<dim3(div_up(count, 128), c.ngroups, 1), 128, 0, s->setup>>>(rows, c.key_mod, nullptr, nullptr,
                                                                                  c.n, c.kcap, c.nkeys, count);
     PowmArgs a;
     a.mod = ArrayView{c.key_mod, c.n, c.kcap, c.kcap, nullptr, 0};
