@@ -192,22 +192,25 @@ xmpError_t XMPAPI xmpIntegersPowmAsync(xmpHandle_t handle, xmpIntegers_t out, co
                                         const xmpIntegers_t exp, const xmpIntegers_t mod, uint32_t count);
 
 /* Allocation-free modular exponentiation (no counterpart in the reference).
- * For callers that cannot allocate device memory: inside a CUDA stream
- * capture, on a latency-critical path where cudaMalloc/cudaFree would
- * synchronise the device, or under another allocator that only hands out the
- * operand buffers.  out[i] = base[i]^exp[i] mod mod[i] for i < count, enqueued
- * on `stream` of the current device; no handle, no cudaMalloc/cudaFree.
+ * For callers that cannot allocate device memory: a latency-critical path
+ * where cudaMalloc/cudaFree would synchronise the device, or a process whose
+ * device memory belongs to another allocator that only hands out the operand
+ * buffers.  out[i] = base[i]^exp[i] mod mod[i] for i < count, enqueued on
+ * `stream` of the current device; no handle, no cudaMalloc/cudaFree.
  * Operands are device pointers (16-byte aligned) in this library's device
  * layout: limb j of instance i at uint32 offset ((j/4)*stride + i)*4 + j%4,
  * stride >= count; base/mod/out have `precision` bits, exp `exp_precision`
- * bits (multiples of 32); moduli odd; out may alias an input.
+ * bits (multiples of 32); moduli odd; out may alias an input.  Limbs move in
+ * whole groups of four, so each buffer must hold ceil(bits/128)*stride*16
+ * bytes (bits = precision, or exp_precision for exp); the padding limbs of
+ * the last group are read as zero and written as zero.
  * Window tables live in a fixed 16 MiB device array that every GPU loading the
  * library holds until exit; batches whose tables do not fit even with the
  * smallest window return xmpErrorIncreaseScratchLimit (split the batch), and
  * precisions above 16,384 bits return xmpErrorUnsupported.  All calls share
  * that array: calls that overlap on the GPU race, so serialise them.  The
- * first call on a device looks up the array's device address; make it before
- * any stream capture. */
+ * first call in each CUDA context looks up the array's device address; make
+ * it before any stream capture. */
 xmpError_t XMPAPI xmpIntegersPowmNoAlloc(cudaStream_t stream, uint32_t *out, const uint32_t *base,
                                           const uint32_t *exp, const uint32_t *mod, uint32_t precision,
                                           uint32_t exp_precision, uint32_t stride, uint32_t count);

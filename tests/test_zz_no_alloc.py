@@ -1,15 +1,16 @@
-"""xmpIntegersPowmNoAlloc against the regular xmpIntegersPowm, through the C ABI.
+"""xmpIntegersPowmNoAlloc against the regular xmpIntegersPowm and GMP, through the C ABI.
 
 The allocation-free entry point serves callers that cannot allocate device
-memory (inside a stream capture, on a latency-critical path where cudaMalloc
-would synchronise the device, or under an allocator that only hands out the
-operand buffers): it keeps its window tables in a fixed device array shared by
-every call.  This test allocates the operand buffers itself (the caller's
-job), runs two different batches in a row through the new entry point and
-requires bit-identical results to the existing entry point for both, so the
-second call cannot be reading stale tables from the first.  It also checks the
-documented size limit.  Kept in its own file, collected last, and independent
-of the other tests' state.
+memory (a latency-critical path where cudaMalloc would synchronise the
+device, or an allocator that only hands out the operand buffers): it keeps
+its window tables in a fixed device array shared by every call.  These tests
+allocate the operand buffers themselves (the caller's job), run two different
+batches in a row through the new entry point and require bit-identical
+results to the existing entry point and to GMP for both, so the second call
+cannot be reading stale tables from the first; they also check the documented
+size limit, a batch large enough that the window must shrink to fit the
+array, and an output that aliases an input.  Kept in their own file, collected
+last, and independent of the other tests' state.
 """
 import ctypes
 
@@ -74,6 +75,8 @@ def test_powm_no_alloc_matches_regular_entry_point_twice():
             torch.cuda.synchronize()
             got = _deinterleave(dout.cpu().numpy().view(np.uint32), count, n, stride)
             assert np.array_equal(got, want), "call %d differs from xmpIntegersPowm" % (call + 1)
+            gmp, _ = oracle.powm(x, e, m, count)
+            assert np.array_equal(got, gmp), "call %d differs from GMP" % (call + 1)
         # sizes beyond the fixed scratch are rejected, nothing is launched
         big = 1 << 16
         rc = lib.xmpIntegersPowmNoAlloc(stream.cuda_stream, dout.data_ptr(), dx.data_ptr(), de.data_ptr(),
@@ -84,3 +87,48 @@ def test_powm_no_alloc_matches_regular_entry_point_twice():
         assert rc == xmp.ERR["xmpErrorInvalidCount"]
     finally:
         h.destroy()
+
+
+def _no_alloc(lib, stream, out, x, e, m, bits, ebits, stride, count):
+    rc = lib.xmpIntegersPowmNoAlloc(stream.cuda_stream, out.data_ptr(), x.data_ptr(), e.data_ptr(), m.data_ptr(),
+                                    bits, ebits, stride, count)
+    assert rc == 0, xmp.XmpError(rc).name
+    torch_sync()
+
+
+def torch_sync():
+    import torch
+    torch.cuda.synchronize()
+
+
+def test_powm_no_alloc_window_shrink_and_aliasing():
+    """4096-bit batch whose default-window tables exceed the 16 MiB array (the window shrinks), then the
+    output written over the exponent and over the base buffers."""
+    import torch
+
+    torch.cuda.set_device(0)
+    lib = xmp.lib()
+    stream = torch.cuda.current_stream()
+    bits, count = 4096, 640
+    n, stride = bits // 32, 640
+    m = oracle.full_length_odd(81, count, n)
+    x = oracle.below(82, m)
+    e = oracle.random_limbs(83, count, n)
+    want, _ = oracle.powm(x, e, m, count)
+    dx, de, dm = (torch.from_numpy(_interleave(v, stride).view(np.int32)).cuda() for v in (x, e, m))
+    dout = torch.zeros_like(dx)
+    _no_alloc(lib, stream, dout, dx, de, dm, bits, bits, stride, count)
+    assert np.array_equal(_deinterleave(dout.cpu().numpy().view(np.uint32), count, n, stride), want)
+    # out == exp
+    _no_alloc(lib, stream, de, dx, de, dm, bits, bits, stride, count)
+    assert np.array_equal(_deinterleave(de.cpu().numpy().view(np.uint32), count, n, stride), want)
+    # out == base (2048 bits, a second shape through the same array)
+    bits, count = 2048, 300
+    n, stride = bits // 32, 320
+    m = oracle.full_length_odd(84, count, n)
+    x = oracle.below(85, m)
+    e = oracle.random_limbs(86, count, n)
+    want, _ = oracle.powm(x, e, m, count)
+    dx, de, dm = (torch.from_numpy(_interleave(v, stride).view(np.int32)).cuda() for v in (x, e, m))
+    _no_alloc(lib, stream, dx, dx, de, dm, bits, bits, stride, count)
+    assert np.array_equal(_deinterleave(dx.cpu().numpy().view(np.uint32), count, n, stride), want)
