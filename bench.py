@@ -199,6 +199,122 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def _timed_events(fn, stream, flush, steps, warmup):
+    """Per-step CUDA-event times (ms) on `stream`, L2 flushed before each step outside the events."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    evs = []
+    for _ in range(steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        evs.append((a, b))
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in evs]
+
+
+def powm_rows(h, x, e, m):
+    """x^e mod m row-wise through xmpIntegersPowm (this library)."""
+    import xmp_b200 as xmp
+    count, n = m.shape
+    X, E, M, O = (h.integers(32 * n, count, v) for v in (x, e, m, None))
+    try:
+        xmp.powm(h, O, X, E, M, count)
+        return O.export()
+    finally:
+        for v in (X, E, M, O):
+            v.destroy()
+
+
+def config1_suite(h, stream, flush, steps, warmup, imad_peak, cpu_seconds):
+    """Plain batched powm, 4,096 independent 1024-bit instances with full-length exponents
+    (seeded like the headline): device-resident modexp/s, IMAD roofline, end to end through
+    the C API with pinned host buffers, GMP on the host, every result checked against GMP."""
+    import torch
+    import oracle as orc
+    import xmp_b200 as xmp
+    bits, count = 1024, 4096
+    n = bits // 32
+    x, e, m = make_inputs(bits, count)
+    lib = xmp.lib()
+    X, E, M, O = (h.integers(bits, count) for _ in range(4))
+    for arr, rows in ((X, x), (E, e), (M, m)):
+        arr.import_(rows)
+    cfg = xmp.powm_get_config(h, bits, bits, count)
+
+    def step():
+        xmp.check(lib.xmpIntegersPowmAsync(h.h, O.x, X.x, E.x, M.x, count), "xmpIntegersPowmAsync")
+
+    ms = statistics.median(_timed_events(step, stream, flush, steps, warmup))
+    hx, he, hm = (torch.from_numpy(v).pin_memory() for v in (x, e, m))
+    hout = torch.empty((count, n), dtype=torch.int32).pin_memory()
+    w = ctypes.c_uint32(0)
+
+    def e2e_step():
+        for arr, buf in ((X, hx), (E, he), (M, hm)):
+            xmp.check(lib.xmpIntegersImportAsync(h.h, arr.x, n, -1, 4, -1, 0, buf.data_ptr(), count), "Import")
+        step()
+        xmp.check(lib.xmpIntegersExportAsync(h.h, hout.data_ptr(), ctypes.byref(w), -1, 4, -1, 0, O.x, count),
+                  "Export")
+
+    e2e_ms = statistics.median(_timed_events(e2e_step, stream, flush, steps, warmup))
+    want, _ = orc.powm(x, e, m, count)
+    ok = bool(np.array_equal(hout.numpy().view(np.uint32), want))
+    rate, used, sample, dt = cpu_gmp_rate(x, e, m, target_s=cpu_seconds)
+    for v in (X, E, M, O):
+        v.destroy()
+    achieved = imad_per_modexp(bits, bits) * count / (ms * 1e-3) / 1e12
+    return {"workload": "batched powm 1024-bit x 4096 instances, full-length exponents",
+            "value": count / (ms * 1e-3), "unit": "modexp/s", "ms_per_step": ms,
+            "kernel": {"lanes": cfg.lanes, "limbs": cfg.limbs, "window": cfg.window},
+            "roofline": {"bound": "imad", "achieved": achieved, "peak": imad_peak, "unit": "TIMAD/s",
+                         "frac": achieved / imad_peak},
+            "e2e": {"value": count / (e2e_ms * 1e-3), "unit": "modexp/s", "h2d_bytes_per_step": 3 * count * n * 4,
+                    "d2h_bytes_per_step": count * n * 4},
+            "cpu_baseline": {"value": rate, "unit": "modexp/s", "cores": used, "kind": "port",
+                             "sample": "%d instances (%.1f s, GMP mpz_powm via OpenMP)" % (sample, dt)},
+            "result_check": ok}
+
+
+def reference_gpu_suite(stream, flush, steps, warmup, ours):
+    """The reference XMP's own kernels on this GPU (oracle/_ref, built from its sources for
+    sm_100a by oracle/build_ref.sh): modexp/s on the headline workload and the 1024-bit x 4,096
+    workload, both variants (-DIMAD and its default XMAD emulation), device-resident operands,
+    CUDA events on the default stream it launches on; results compared with this library's
+    (`ours`: {(bits, count): rows})."""
+    import torch
+    from oracle import ref_xmp
+    out = {}
+    for variant in ("imad", "xmad"):
+        if not ref_xmp.available(variant):
+            out[variant] = {"unavailable": "oracle/_ref/libxmp_ref_%s.so not built" % variant}
+            continue
+        r = ref_xmp.Ref(variant)
+        res = {}
+        try:
+            for (bits, count), rows in ours.items():
+                x, e, m = make_inputs(bits, count)
+                O, X, E, M = r.powm_arrays(x, e, m)
+                dflt = torch.cuda.default_stream()
+                with torch.cuda.stream(dflt):
+                    ms = statistics.median(_timed_events(lambda: r.powm_async(O, X, E, M, count), dflt, flush,
+                                                         steps, warmup))
+                got = r.export(O, bits, count)
+                res["%d_x_%d" % (bits, count)] = {"value": count / (ms * 1e-3), "unit": "modexp/s",
+                                                  "ms_per_step": ms,
+                                                  "identical_to_ours": bool(np.array_equal(got, rows))}
+                r.close()
+                r = ref_xmp.Ref(variant)
+        finally:
+            r.close()
+        out[variant] = res
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import xmp_b200 as xmp
@@ -315,6 +431,22 @@ def run_ours(args, rank, world, local_rank):
                "sample": "%d instances of the same workload (%.1f s, GMP mpz_powm via OpenMP)" % (sample, dt),
                "single_core": {"value": rate1, "sample": "%d instances (%.1f s, 1 thread)" % (sample1, dt1)}}
 
+    extra = None
+    if world == 1 and not args.no_extra:
+        # the other single-GPU workloads, measured after the headline's timed regions (rank 0, N = 1)
+        t0 = time.perf_counter()
+        extra = {}
+        extra["config1_1024bit_x4096"] = config1_suite(h, stream, flush, args.steps, args.warmup, peaks["imad"],
+                                                       min(args.cpu_seconds, 3.0))
+        xx, ee, mm = make_inputs(1024, 4096)
+        ours1 = {(bits, count): res.copy(), (1024, 4096): powm_rows(h, xx, ee, mm)}
+        extra["reference_gpu"] = reference_gpu_suite(stream, flush, 3, 1, ours1)
+        ew, ew_cpu, hbm = elementwise_suite(h, stream, 5, 2, peaks["imad"])
+        extra["config2_elementwise"] = {"ops": ew, "cpu_baseline_ops_per_s": ew_cpu, "hbm_peak_gbs": hbm,
+                                        "imad_peak_timad_s": peaks["imad"]}
+        extra["config3_mixed"] = mixed_suite(3, 1, 65536, 16384, 256)
+        extra["seconds"] = time.perf_counter() - t0
+
     line = {
         "metric": "%d-bit modexp/s" % bits, "value": value, "unit": "modexp/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -331,6 +463,8 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": args.steps,
         "result_check": check_ok,
     }
+    if extra is not None:
+        line["extra_configs"] = extra
     print(json.dumps(line), flush=True)
     for v in (X, E, M, O):
         v.destroy()
@@ -353,18 +487,19 @@ def _crt_keys(nkeys, half_bits, seed):
     return keys
 
 
-def run_mixed(args):
+def mixed_suite(steps, warmup, total, ncrt, nkeys):
     """Uneven-size batch: 65,536 instances (40% 1024, 30% 2048, 20% 3072, 10% 4096 bits,
     full-length exponents, bases in [0, m)) plus 16,384 CRT-RSA private operations
     (1024-bit primes from nextprime, e = 65537, Garner with q^-1 mod p, messages
     uniform in [0, pq)).  Plain per-size xmpIntegersPowm calls and the CRT op
-    sequence vs one autotuned batch plan replayed as a CUDA graph."""
+    sequence -- with the library's default (compiled-in selector) choices and with
+    the static heuristic alone (a handle whose tuner is cleared) -- vs one
+    autotuned batch plan replayed as a CUDA graph.  Returns the result dict."""
     import torch
     import oracle as orc
     import xmp_b200 as xmp
     from xmp_b200 import tuning
     torch.cuda.set_device(0)
-    total, ncrt, nkeys = args.count, args.crt, args.crt_keys
     mix = [(1024, 0.4), (2048, 0.3), (3072, 0.2), (4096, 0.1)]
     sizes = [(b, int(total * f)) for b, f in mix]
     sizes[0] = (1024, total - sum(c for _, c in sizes[1:]))
@@ -397,7 +532,11 @@ def run_mixed(args):
                mq=h.integers(1024, ncrt), p2=h.integers(1056, nkeys), t1=h.integers(1056, ncrt),
                d=h.integers(1056, ncrt), e=h.integers(2080, ncrt), hh=h.integers(1024, ncrt), f=h.integers(2048, ncrt))
 
-    def plain():
+    heur = xmp.Handle()  # the static register/occupancy heuristic only
+    heur.set_stream(stream.cuda_stream)
+    xmp.check(xmp.lib().xmpTuneClear(heur.h), "xmpTuneClear")
+
+    def plain(h=h):
         for g in groups:
             xmp.check(xmp.lib().xmpIntegersPowmAsync(h.h, g["O1"].x, g["X"].x, g["E"].x, g["M"].x, g["count"]))
         L = xmp.lib()
@@ -433,8 +572,9 @@ def run_mixed(args):
         return float(np.median(ts))
 
     # plain launches use the library's default choices (the compiled-in selector), as any caller gets
-    t_plain = timed(plain, args.steps, args.warmup)
-    t_batch = timed(plan.execute, args.steps, args.warmup)
+    t_plain = timed(plain, steps, warmup)
+    t_heur = timed(lambda: plain(heur), steps, warmup)
+    t_batch = timed(plan.execute, steps, warmup)
     # the plain launches one at a time: their sum bounds what any schedule of the same kernels can gain
     parts = {}
     for g in groups:
@@ -448,20 +588,30 @@ def run_mixed(args):
     want, _ = orc.powm(x, e, m, len(m))
     ok = ok and np.array_equal(groups[1]["O2"].export()[:16], want)
     n_ops = total + ncrt
-    line = {"metric": "mixed-size batch speedup (autotuned batch plan vs plain per-size launches)",
-            "value": t_plain / t_batch, "unit": "x", "higher_is_better": True, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_batch, "dtype": "u32", "data": "synthetic (seeded)",
-            "config": {"workload": "65,536 mixed powm (40/30/20/10%% of 1024/2048/3072/4096 bits) + %d CRT-RSA-2048"
-                       % ncrt, "crt_keys": nkeys, "selector": selector},
-            "plain_ms": t_plain, "batch_ms": t_batch, "plain_parts_ms": parts, "plain_ops_per_s": n_ops / (t_plain * 1e-3),
-            "batch_ops_per_s": n_ops / (t_batch * 1e-3),
-            "bins": [dict(precision=b["precision"], count=b["count"], blocks=b["blocks"],
-                          lanes=b["config"].lanes, limbs=b["config"].limbs, window=b["config"].window)
-                     for b in plan.info()],
-            "result_check": ok}
-    print(json.dumps(line), flush=True)
+    out = {"speedup_vs_plain_selector": t_plain / t_batch, "speedup_vs_plain_heuristic": t_heur / t_batch,
+           "plain_ms": t_plain, "plain_heuristic_ms": t_heur, "batch_ms": t_batch, "plain_parts_ms": parts,
+           "plain_ops_per_s": n_ops / (t_plain * 1e-3), "batch_ops_per_s": n_ops / (t_batch * 1e-3),
+           "bins": [dict(precision=b["precision"], count=b["count"], blocks=b["blocks"],
+                         lanes=b["config"].lanes, limbs=b["config"].limbs, window=b["config"].window)
+                    for b in plan.info()],
+           "selector": selector, "result_check": ok}
     plan.destroy()
+    heur.destroy()
     h.destroy()
+    return out
+
+
+def run_mixed(args):
+    """The mixed-size batch (mixed_suite) as its own JSON line."""
+    r = mixed_suite(args.steps, args.warmup, args.count, args.crt, args.crt_keys)
+    line = {"metric": "mixed-size batch speedup (autotuned batch plan vs plain per-size launches)",
+            "value": r["speedup_vs_plain_selector"], "unit": "x", "higher_is_better": True, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["batch_ms"], "dtype": "u32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": "65,536 mixed powm (40/30/20/10%% of 1024/2048/3072/4096 bits) + %d CRT-RSA-2048"
+                       % args.crt, "crt_keys": args.crt_keys, "selector": r["selector"]}}
+    line.update({k: v for k, v in r.items() if k != "selector"})
+    print(json.dumps(line), flush=True)
 
 
 def run_serve(args):
@@ -573,7 +723,7 @@ def run_serve(args):
     h.destroy()
 
 
-def run_elementwise(args):
+def elementwise_suite(h, stream, steps, warmup, imad_peak):
     """Elementwise and contraction suite: add, sub, and, ior, xor, not, shf (shifts
     uniform 0..255), cmp, popc on 2^22 pairs of 256-bit operands (HBM-bound:
     GB/s of algorithmic bytes against the measured HBM copy bandwidth); mul on
@@ -581,14 +731,10 @@ def run_elementwise(args):
     dividends by 1024-bit divisors with the top bit set.  Operands resident in
     HBM (every working set exceeds the 126 MB L2); each op checked bit-exact
     against GMP on its first 4,096 instances; GMP multithreaded on the host
-    for add, mul and divmod."""
+    for add, mul and divmod.  Returns (per-op results, GMP rates, HBM peak)."""
     import torch
     import oracle as orc
     import xmp_b200 as xmp
-    torch.cuda.set_device(0)
-    h = xmp.Handle()
-    stream = torch.cuda.current_stream()
-    h.set_stream(stream.cuda_stream)
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -596,7 +742,6 @@ def run_elementwise(args):
     except (OSError, ValueError):
         pass
     hbm = peaks.get("hbm_gbs") or 6650.0
-    imad_peak = probe_imad_peak()["imad"]
     E = 1 << 22
     a = orc.random_limbs(31, E, 8)
     b = orc.random_limbs(32, E, 8)
@@ -611,11 +756,11 @@ def run_elementwise(args):
         """Median device time of one call.  Every step is queued behind an L2
         flush (a 252 MB write), so the GPU never waits for the host inside the
         events and no step finds its operands in L2; one synchronize at the end."""
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             fn()
         torch.cuda.synchronize()
         evs = []
-        for _ in range(args.steps):
+        for _ in range(steps):
             flush.zero_()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -698,6 +843,20 @@ def run_elementwise(args):
     cpu["divmod"] = M / (time.perf_counter() - t)
     for X in (DA, DB, DQ, DR):
         X.destroy()
+    return res, cpu, hbm
+
+
+def run_elementwise(args):
+    """The elementwise and contraction suite (elementwise_suite) as its own JSON line."""
+    import torch
+    import oracle as orc
+    import xmp_b200 as xmp
+    torch.cuda.set_device(0)
+    h = xmp.Handle()
+    stream = torch.cuda.current_stream()
+    h.set_stream(stream.cuda_stream)
+    imad_peak = probe_imad_peak()["imad"]
+    res, cpu, hbm = elementwise_suite(h, stream, args.steps, args.warmup, imad_peak)
     line = {"metric": "elementwise suite HBM GB/s (256-bit add)", "value": res["add"]["gbs"], "unit": "GB/s",
             "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": res["add"]["ms"], "dtype": "u32", "data": "synthetic (seeded splitmix64 limbs)",
@@ -724,6 +883,7 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="headline workload only (no config 1/2/3 or reference GPU)")
     ap.add_argument("--force-config", default=None, help="lanes,limbs,window: time this powm kernel configuration")
     ap.add_argument("--workload", default="powm2048", choices=["powm2048", "mixed", "serve", "elementwise"])
     ap.add_argument("--serve-seconds", type=float, default=1.0)

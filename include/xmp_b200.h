@@ -73,6 +73,28 @@ typedef struct {
 
 typedef struct _xmpPowmBatchPlan_t *xmpPowmBatchPlan_t;
 
+/* ---- fused CRT-RSA private operation -----------------------------------------
+ * (no counterpart in the reference library; replaces the op sequence of its
+ * CRT-RSA sample, samples/crt_rsa/rsa.cc:206-219: c mod p, c mod q, two powm,
+ * two mul, add, mod.)  out[i] = c[i]^d mod p*q for i < count, computed from
+ * p, q, dp = d mod (p-1), dq = d mod (q-1) and qinv = q^-1 mod p in one
+ * kernel launch: Montgomery reductions of c, the two half-size
+ * exponentiations with a fixed window over the whole precision of dp and dq
+ * (the same sequence of multiplications whatever the exponent bits), and
+ * Garner's recombination mq + q*((mp - mq)*qinv mod p).  p, q and qinv have
+ * one precision h (p and q odd, qinv < p); out has 2h bits; c at most 2h bits
+ * and below p*q; dp and dq any precision.  Every input is broadcast like an
+ * XMP operand (element i % its count); the handle's index policy is not used.
+ * The window tables use the handle's scratch arena (the batch is chunked to
+ * its limit). */
+xmpError_t XMPAPI xmpIntegersPowmCRT(xmpHandle_t handle, xmpIntegers_t out, const xmpIntegers_t c,
+                                     const xmpIntegers_t p, const xmpIntegers_t q, const xmpIntegers_t dp,
+                                     const xmpIntegers_t dq, const xmpIntegers_t qinv, uint32_t count);
+xmpError_t XMPAPI xmpIntegersPowmCRTAsync(xmpHandle_t handle, xmpIntegers_t out, const xmpIntegers_t c,
+                                          const xmpIntegers_t p, const xmpIntegers_t q, const xmpIntegers_t dp,
+                                          const xmpIntegers_t dq, const xmpIntegers_t qinv, uint32_t count);
+
+
 xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t handle, const xmpPowmBatchItem_t *items, int32_t n_items,
                                          const xmpPowmCRTItem_t *crt, int32_t n_crt, int32_t use_graph,
                                          xmpPowmBatchPlan_t *plan);

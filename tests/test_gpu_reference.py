@@ -29,6 +29,16 @@ def ref():
     r.close()
 
 
+@pytest.fixture(scope="module")
+def ref_xmad():
+    """The reference's default build (16-bit XMAD multiply emulation)."""
+    if not ref_xmp.available("xmad"):
+        pytest.skip("reference XMAD variant not built")
+    r = ref_xmp.Ref("xmad")
+    yield r
+    r.close()
+
+
 def _ours_powm(h, x, e, m):
     count, n = m.shape
     X, E, M, O = h.integers(32 * n, count, x), h.integers(32 * e.shape[1], count, e), h.integers(32 * n, count, m), \
@@ -63,6 +73,13 @@ def test_powm_config1_exact(handle, ref):
     assert np.array_equal(ours, theirs)
     want, _ = oracle.powm(x, e, m, 4096)
     assert np.array_equal(ours, want)
+
+
+def test_powm_xmad_variant(handle, ref_xmad):
+    """The reference's default XMAD build gives the same results (1024 and 2048 bits)."""
+    for bits, count in ((1024, 512), (2048, 256)):
+        x, e, m = _inputs(700 + bits, bits, count)
+        assert np.array_equal(_ours_powm(handle, x, e, m), ref_xmad.powm(x, e, m)), bits
 
 
 @pytest.mark.parametrize("bits,count", [(2048, 1024), (1536, 512)])

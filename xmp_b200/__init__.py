@@ -85,6 +85,8 @@ _SIGS = {
     "xmpIntegersPowm": [_VP, _VP, _VP, _VP, _VP, _U32],
     "xmpIntegersPowmAsync": [_VP, _VP, _VP, _VP, _VP, _U32],
     "xmpIntegersPowmNoAlloc": [_VP, _VP, _VP, _VP, _VP, _U32, _U32, _U32, _U32],
+    "xmpIntegersPowmCRT": [_VP] * 8 + [_U32],
+    "xmpIntegersPowmCRTAsync": [_VP] * 8 + [_U32],
     "xmpPowmKernelCount": [ctypes.POINTER(_I32)],
     "xmpPowmKernelGet": [_I32, ctypes.POINTER(_I32), ctypes.POINTER(_I32)],
     "xmpPowmGetConfig": [_VP, _U32, _U32, _U32, _VP],
@@ -448,6 +450,12 @@ class Server:
 def powm(h, out, base, exp, mod_, count, asynchronous=False):
     fn = lib().xmpIntegersPowmAsync if asynchronous else lib().xmpIntegersPowm
     check(fn(h.h, _x(out), _x(base), _x(exp), _x(mod_), count), "xmpIntegersPowm")
+
+
+def powm_crt(h, out, c, p, q, dp, dq, qinv, count, asynchronous=False):
+    """out = c^d mod pq from the CRT key (p, q, dp, dq, qinv) in one fused kernel (xmpIntegersPowmCRT)."""
+    fn = lib().xmpIntegersPowmCRTAsync if asynchronous else lib().xmpIntegersPowmCRT
+    check(fn(h.h, _x(out), _x(c), _x(p), _x(q), _x(dp), _x(dq), _x(qinv), count), "xmpIntegersPowmCRT")
 
 
 def shf(h, c, a, shifts, count, shift_count=None):

@@ -2,17 +2,17 @@
 // reference, whose xmpIntegersPowm handles one precision per call through a
 // host chunk loop, src/powm.cu:250-307).
 //
-// A plan bins instances by modulus precision.  Each bin is one persistent
-// powm_batch_kernel launch: a fixed number of CTAs -- the bin's share of the
-// GPU, proportional to its work -- whose warps pull work items from an atomic
-// queue spanning up to kPowmSegs segments, so CRT half-exponentiations run in
-// the same kernel as plain instances of their precision.  Bins are forked
-// onto side streams and joined back, so all of them run concurrently; CRT
-// reductions (c mod p, c mod q) run before the fork and the Garner
-// recombination right after the bin holding the CRT halves.  Everything is
-// sized and allocated at plan creation, so the execution can be captured into
-// one CUDA graph and replayed.
+// A plan bins plain instances by modulus precision.  Each bin is one
+// persistent powm_batch_kernel launch: a full grid whose warps pull work items
+// from an atomic queue spanning up to kPowmSegs segments (arrays of the same
+// precision).  CRT-RSA items run as one fused crt_kernel launch each (c mod p
+// and mod q, both half exponentiations and Garner's recombination in one
+// kernel, no temporaries; crt.cuh).  Bins and CRT launches are forked onto
+// side streams and joined back, so all of them run concurrently.  Everything
+// is sized and allocated at plan creation, so the execution can be captured
+// into one CUDA graph and replayed.
 #include "tune.h"
+#include "crt.h"
 #include <algorithm>
 #include <vector>
 
@@ -33,20 +33,20 @@ struct BatchBin {
   int blocks = 0;
   bool serial = false;  // digit-serial fallback, run after the join
   size_t table_offset = 0;
-  bool has_crt = false;
 };
 
-struct CrtTemps {
-  xmpIntegers_t cp = nullptr, cq = nullptr, mp = nullptr, mq = nullptr, p2 = nullptr, t1 = nullptr, d = nullptr,
-                e = nullptr, hh = nullptr, f = nullptr;
+struct CrtLaunch {
+  xmpPowmCRTItem_t item;
+  CrtConfig cfg;
+  uint32_t chunk = 0;
+  size_t table_offset = 0;
 };
 
 }  // namespace xmpb
 
 struct _xmpPowmBatchPlan_t {
   std::vector<BatchBin> bins;
-  std::vector<xmpPowmCRTItem_t> crt;
-  std::vector<CrtTemps> temps;
+  std::vector<CrtLaunch> crt;
   void *scratch = nullptr;
   size_t scratch_bytes = 0;
   uint32_t *counters = nullptr;
@@ -61,16 +61,9 @@ struct _xmpPowmBatchPlan_t {
 
 namespace xmpb {
 
-static xmpError_t make(xmpHandle_t h, xmpIntegers_t *x, uint32_t bits, uint32_t count) {
-  return xmpIntegersCreate(h, x, bits, count);
-}
-
 static void free_plan(xmpHandle_t h, xmpPowmBatchPlan_t p) {
   if (p->exec) cudaGraphExecDestroy(p->exec);
   if (p->graph) cudaGraphDestroy(p->graph);
-  for (auto &t : p->temps)
-    for (xmpIntegers_t x : {t.cp, t.cq, t.mp, t.mq, t.p2, t.t1, t.d, t.e, t.hh, t.f})
-      if (x) xmpIntegersDestroy(h, x);
   if (p->scratch) h->df(p->scratch);
   for (auto s : p->side) cudaStreamDestroy(s);
   for (auto e : p->joins) cudaEventDestroy(e);
@@ -122,36 +115,26 @@ static xmpError_t enqueue(xmpHandle_t h, xmpPowmBatchPlan_t p, cudaStream_t main
   auto run = [&]() -> xmpError_t {
     xmpError_t r;
     if (cudaMemsetAsync(p->counters, 0, p->bins.size() * sizeof(uint32_t), main) != cudaSuccess) return xmpErrorCuda;
-    for (size_t c = 0; c < p->crt.size(); c++) {
-      const xmpPowmCRTItem_t &it = p->crt[c];
-      if ((r = xmpIntegersModAsync(h, p->temps[c].cp, it.c, it.p, it.count))) return r;
-      if ((r = xmpIntegersModAsync(h, p->temps[c].cq, it.c, it.q, it.count))) return r;
-    }
     if (cudaEventRecord(p->fork, main) != cudaSuccess) return xmpErrorCuda;
-    // every bin on its own stream, in launch order (longest instances first);
-    // the Garner recombination follows the bin holding the CRT halves
+    // every bin and every CRT item on its own stream, in launch order (longest instances first)
     int side = 0;
     for (size_t b = 0; b < p->bins.size(); b++) {
       if (p->bins[b].serial) continue;
       cudaStream_t s = p->side[side];
       if (cudaStreamWaitEvent(s, p->fork, 0) != cudaSuccess) return xmpErrorCuda;
       if ((r = launch_bin(h, p, (int)b, s))) return r;
-      if (p->bins[b].has_crt) {
-        h->stream = s;
-        for (size_t c = 0; c < p->crt.size(); c++) {
-          const xmpPowmCRTItem_t &it = p->crt[c];
-          const CrtTemps &t = p->temps[c];
-          const uint32_t n = it.count;
-          if ((r = xmpIntegersAddAsync(h, t.p2, it.p, it.p, n))) return r;    // 2p
-          if ((r = xmpIntegersAddAsync(h, t.t1, t.mp, t.p2, n))) return r;    // mp + 2p
-          if ((r = xmpIntegersSubAsync(h, t.d, t.t1, t.mq, n))) return r;     // mp + 2p - mq in (0, 3p)
-          if ((r = xmpIntegersMulAsync(h, t.e, t.d, it.qinv, n))) return r;   // d * qinv
-          if ((r = xmpIntegersModAsync(h, t.hh, t.e, it.p, n))) return r;     // h = d * qinv mod p
-          if ((r = xmpIntegersMulAsync(h, t.f, it.q, t.hh, n))) return r;     // q * h
-          if ((r = xmpIntegersAddAsync(h, it.out, t.f, t.mq, n))) return r;   // mq + q * h
-        }
-        h->stream = main;
-      }
+      if (cudaEventRecord(p->joins[side], s) != cudaSuccess) return xmpErrorCuda;
+      side++;
+    }
+    for (const CrtLaunch &c : p->crt) {
+      cudaStream_t s = p->side[side];
+      if (cudaStreamWaitEvent(s, p->fork, 0) != cudaSuccess) return xmpErrorCuda;
+      const xmpPowmCRTItem_t &it = c.item;
+      CrtArgs a = crt_args(it.out, it.out->limbs, it.c, it.p, it.q, it.dp, it.dq, it.qinv);
+      a.window = (uint32_t)c.cfg.window;
+      a.table = (uint32_t *)((char *)p->scratch + c.table_offset);
+      crt_launch(c.cfg, a, it.count, c.chunk, s);
+      if ((r = check_cuda())) return r;
       if (cudaEventRecord(p->joins[side], s) != cudaSuccess) return xmpErrorCuda;
       side++;
     }
@@ -193,7 +176,6 @@ xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t h, const xmpPowmBatchItem_t
   };
   // ---- validate and collect segments ----
   std::vector<BatchSegment> segs;
-  std::vector<bool> seg_is_crt;
   for (int32_t i = 0; i < n_items; i++) {
     const xmpPowmBatchItem_t &it = items[i];
     if (!it.out || !it.base || !it.exp || !it.mod) return fail(xmpErrorInvalidParameter);
@@ -204,36 +186,22 @@ xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t h, const xmpPowmBatchItem_t
     for (xmpIntegers_t x : {it.out, it.base, it.exp, it.mod})
       if (x->device != h->device) return fail(xmpErrorInvalidDevice);
     segs.push_back(BatchSegment{it.out, it.base, it.exp, it.mod, it.count});
-    seg_is_crt.push_back(false);
   }
   for (int32_t i = 0; i < n_crt; i++) {
     const xmpPowmCRTItem_t &it = crt[i];
     if (!it.out || !it.c || !it.p || !it.q || !it.dp || !it.dq || !it.qinv) return fail(xmpErrorInvalidParameter);
     if (it.count == 0) continue;
-    const uint32_t hb = it.p->precision;
-    if (it.q->precision != hb || it.qinv->precision != hb || it.out->precision != 2 * hb || it.c->precision > 2 * hb)
-      return fail(xmpErrorInvalidPrecision);
-    if (it.out->count < it.count) return fail(xmpErrorInvalidCount);
-    p->crt.push_back(it);
-    CrtTemps t;
-    const uint32_t n = it.count;
-    if ((e = make(h, &t.cp, hb, n)) || (e = make(h, &t.cq, hb, n)) || (e = make(h, &t.mp, hb, n)) ||
-        (e = make(h, &t.mq, hb, n)) || (e = make(h, &t.p2, hb + 32, n)) || (e = make(h, &t.t1, hb + 32, n)) ||
-        (e = make(h, &t.d, hb + 32, n)) || (e = make(h, &t.e, 2 * hb + 32, n)) || (e = make(h, &t.hh, hb, n)) ||
-        (e = make(h, &t.f, 2 * hb, n))) {
-      p->temps.push_back(t);
-      return fail(e);
-    }
-    p->temps.push_back(t);
-    segs.push_back(BatchSegment{t.mp, t.cp, it.dp, it.p, n});
-    seg_is_crt.push_back(true);
-    segs.push_back(BatchSegment{t.mq, t.cq, it.dq, it.q, n});
-    seg_is_crt.push_back(true);
+    if ((e = crt_validate(h, it.out, it.c, it.p, it.q, it.dp, it.dq, it.qinv, it.count))) return fail(e);
+    CrtLaunch c;
+    c.item = it;
+    c.cfg = crt_config(it.p->nlimbs, std::max(it.dp->precision, it.dq->precision), it.count, h->sm_count);
+    if (!c.cfg.launch) return fail(xmpErrorUnsupported);
+    c.chunk = it.count;
+    p->crt.push_back(c);
   }
-  // ---- bins: one per precision, at most kPowmSegs segments each; CRT halves first ----
-  for (int pass = 0; pass < 2; pass++) {
+  // ---- bins: one per precision, at most kPowmSegs segments each ----
+  {
     for (size_t i = 0; i < segs.size(); i++) {
-      if (seg_is_crt[i] != (pass == 0)) continue;
       const BatchSegment &s = segs[i];
       BatchBin *bin = nullptr;
       for (auto &b : p->bins)
@@ -246,7 +214,6 @@ xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t h, const xmpPowmBatchItem_t
       bin->segs.push_back(s);
       bin->count += s.count;
       bin->exp_bits = std::max(bin->exp_bits, s.exp->precision);
-      bin->has_crt |= seg_is_crt[i];
     }
   }
   // ---- configurations and grids ----
@@ -307,6 +274,19 @@ xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t h, const xmpPowmBatchItem_t
     bytes += (size_t)b.blocks * 128 * b.cfg.limbs * 4 * powm_table_entries(b.cfg.window, powm_sliding(b.cfg.tpi, b.cfg.limbs));
     bytes = (bytes + 255) & ~(size_t)255;
   }
+  // CRT items: window tables for all instances at once, or chunks of what half the scratch limit holds
+  for (auto &c : p->crt) {
+    const size_t per_inst = (size_t)c.cfg.tpi * c.cfg.limbs * ((size_t)1 << c.cfg.window) * 4;
+    const uint32_t per_block = 128 / c.cfg.tpi;
+    while (c.cfg.window > 1 && per_inst * per_block > scratch_limit(h) / 2) c.cfg.window--;
+    const size_t per = (size_t)c.cfg.tpi * c.cfg.limbs * ((size_t)1 << c.cfg.window) * 4;
+    uint64_t fit = (scratch_limit(h) / 2) / per / per_block * per_block;
+    if (fit < per_block) return fail(xmpErrorIncreaseScratchLimit);
+    c.chunk = (uint32_t)std::min<uint64_t>(c.item.count, fit);
+    c.table_offset = bytes;
+    bytes += crt_table_bytes(c.cfg, c.chunk);
+    bytes = (bytes + 255) & ~(size_t)255;
+  }
   size_t counter_offset = bytes;
   bytes += 256;
   p->scratch = h->da(bytes);
@@ -316,8 +296,8 @@ xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t h, const xmpPowmBatchItem_t
   if (p->bins.size() > 64) return fail(xmpErrorUnsupported);
   // ---- streams and events ----
   if (cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) != cudaSuccess) return fail(xmpErrorCuda);
-  for (size_t b = 0; b < p->bins.size(); b++) {
-    if (p->bins[b].serial) continue;
+  for (size_t b = 0; b < p->bins.size() + p->crt.size(); b++) {
+    if (b < p->bins.size() && p->bins[b].serial) continue;
     cudaStream_t s;
     cudaEvent_t ev;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return fail(xmpErrorCuda);
@@ -325,8 +305,6 @@ xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t h, const xmpPowmBatchItem_t
     if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return fail(xmpErrorCuda);
     p->joins.push_back(ev);
   }
-  // CRT ops may need the handle's scratch (sized now, outside any capture)
-  if ((e = ensure_scratch(h, 1 << 20))) return fail(e);
   if (p->use_graph) {
     if (cudaStreamCreateWithFlags(&p->capture, cudaStreamNonBlocking) != cudaSuccess) return fail(xmpErrorCuda);
     // Run once eagerly so every lazily-sized buffer is in place before capture.
