@@ -575,6 +575,28 @@ def mixed_suite(steps, warmup, total, ncrt, nkeys):
     t_plain = timed(plain, steps, warmup)
     t_heur = timed(lambda: plain(heur), steps, warmup)
     t_batch = timed(plan.execute, steps, warmup)
+    # the CRT part alone: the op sequence above vs one fused xmpIntegersPowmCRT launch
+    L = xmp.lib()
+    crt_out = h.integers(2048, ncrt)
+
+    def crt_seq():
+        xmp.check(L.xmpIntegersModAsync(h.h, tmp["cp"].x, C.x, ka["p"].x, ncrt))
+        xmp.check(L.xmpIntegersModAsync(h.h, tmp["cq"].x, C.x, ka["q"].x, ncrt))
+        xmp.check(L.xmpIntegersPowmAsync(h.h, tmp["mp"].x, tmp["cp"].x, ka["dp"].x, ka["p"].x, ncrt))
+        xmp.check(L.xmpIntegersPowmAsync(h.h, tmp["mq"].x, tmp["cq"].x, ka["dq"].x, ka["q"].x, ncrt))
+        xmp.check(L.xmpIntegersAddAsync(h.h, tmp["p2"].x, ka["p"].x, ka["p"].x, nkeys))
+        xmp.check(L.xmpIntegersAddAsync(h.h, tmp["t1"].x, tmp["mp"].x, tmp["p2"].x, ncrt))
+        xmp.check(L.xmpIntegersSubAsync(h.h, tmp["d"].x, tmp["t1"].x, tmp["mq"].x, ncrt))
+        xmp.check(L.xmpIntegersMulAsync(h.h, tmp["e"].x, tmp["d"].x, ka["qinv"].x, ncrt))
+        xmp.check(L.xmpIntegersModAsync(h.h, tmp["hh"].x, tmp["e"].x, ka["p"].x, ncrt))
+        xmp.check(L.xmpIntegersMulAsync(h.h, tmp["f"].x, ka["q"].x, tmp["hh"].x, ncrt))
+        xmp.check(L.xmpIntegersAddAsync(h.h, outs[0].x, tmp["f"].x, tmp["mq"].x, ncrt))
+
+    t_crt_seq = timed(crt_seq, steps, warmup)
+    t_crt_fused = timed(lambda: xmp.powm_crt(h, crt_out, C, ka["p"], ka["q"], ka["dp"], ka["dq"], ka["qinv"], ncrt,
+                                             asynchronous=True), steps, warmup)
+    crt_ok = [orc.to_int(r) for r in crt_out.export()[:256]] == msgs[:256]
+    crt_out.destroy()
     # the plain launches one at a time: their sum bounds what any schedule of the same kernels can gain
     parts = {}
     for g in groups:
@@ -589,6 +611,8 @@ def mixed_suite(steps, warmup, total, ncrt, nkeys):
     ok = ok and np.array_equal(groups[1]["O2"].export()[:16], want)
     n_ops = total + ncrt
     out = {"speedup_vs_plain_selector": t_plain / t_batch, "speedup_vs_plain_heuristic": t_heur / t_batch,
+           "crt_rsa2048_x%d" % ncrt: {"op_sequence_ms": t_crt_seq, "fused_kernel_ms": t_crt_fused,
+                                      "speedup": t_crt_seq / t_crt_fused, "fused_result_check": crt_ok},
            "plain_ms": t_plain, "plain_heuristic_ms": t_heur, "batch_ms": t_batch, "plain_parts_ms": parts,
            "plain_ops_per_s": n_ops / (t_plain * 1e-3), "batch_ops_per_s": n_ops / (t_batch * 1e-3),
            "bins": [dict(precision=b["precision"], count=b["count"], blocks=b["blocks"],
@@ -726,7 +750,8 @@ def run_serve(args):
 def elementwise_suite(h, stream, steps, warmup, imad_peak):
     """Elementwise and contraction suite: add, sub, and, ior, xor, not, shf (shifts
     uniform 0..255), cmp, popc on 2^22 pairs of 256-bit operands (HBM-bound:
-    GB/s of algorithmic bytes against the measured HBM copy bandwidth); mul on
+    GB/s of algorithmic bytes against the measured HBM copy bandwidth, and against
+    a device-to-device copy of the same byte count timed the same way); mul on
     2^18 pairs of 512 x 512 -> 1024 bits; divmod on 2^18 instances of 2048-bit
     dividends by 1024-bit divisors with the top bit set.  Operands resident in
     HBM (every working set exceeds the 126 MB L2); each op checked bit-exact
@@ -772,11 +797,25 @@ def elementwise_suite(h, stream, steps, warmup, imad_peak):
 
     S = 4096
     res = {}
+    copies = {}
 
-    def row(name, ms, bytes_per_op, count, ok, imad_per_op=0):
+    def copy_gbs(total):
+        """GB/s of a device-to-device copy moving `total` bytes (read + write), timed like the ops:
+        the bandwidth a launch of this size reaches, launch and ramp included."""
+        if total not in copies:
+            src = torch.empty(total // 2, dtype=torch.uint8, device="cuda")
+            dst = torch.empty_like(src)
+            copies[total] = total / (timed(lambda: dst.copy_(src)) * 1e-3) / 1e9
+            del src, dst
+        return copies[total]
+
+    def row(name, ms, bytes_per_op, count, ok, imad_per_op=0, vs_copy=False):
         r = {"ms": ms, "ops_per_s": count / (ms * 1e-3), "bytes_per_op": bytes_per_op,
              "gbs": bytes_per_op * count / (ms * 1e-3) / 1e9, "check": bool(ok)}
         r["hbm_frac"] = r["gbs"] / hbm
+        if vs_copy:
+            r["copy_gbs_same_bytes"] = copy_gbs(bytes_per_op * count)
+            r["copy_frac"] = r["gbs"] / r["copy_gbs_same_bytes"]
         if imad_per_op:
             r["timad_s"] = imad_per_op * count / (ms * 1e-3) / 1e12
             r["imad_frac"] = r["timad_s"] / imad_peak
@@ -786,16 +825,17 @@ def elementwise_suite(h, stream, steps, warmup, imad_peak):
                          ("ior", xmp.ior, "ior"), ("xor", xmp.xor, "xor")):
         ms = timed(lambda fn=fn: fn(h, C, A, B, E, asynchronous=True))
         ok = np.array_equal(C.export(count=E)[:S], orc.binary(op, a[:S], b[:S], 8, S))
-        row(name, ms, 96, E, ok)
+        row(name, ms, 96, E, ok, vs_copy=True)
     ms = timed(lambda: xmp.not_(h, C, A, E, asynchronous=True))
-    row("not", ms, 64, E, np.array_equal(C.export()[:S], orc.not_(a[:S], 8, S)))
+    row("not", ms, 64, E, np.array_equal(C.export()[:S], orc.not_(a[:S], 8, S)), vs_copy=True)
     L = xmp.lib()
     ms = timed(lambda: xmp.check(L.xmpIntegersShfAsync(h.h, C.x, A.x, SH.data_ptr(), E, E)))
-    row("shf", ms, 68, E, np.array_equal(C.export()[:S], orc.shf(a[:S], sh[:S], 8, S)))
+    row("shf", ms, 68, E, np.array_equal(C.export()[:S], orc.shf(a[:S], sh[:S], 8, S)), vs_copy=True)
     ms = timed(lambda: xmp.check(L.xmpIntegersCmpAsync(h.h, I32.data_ptr(), A.x, B.x, E)))
     row("cmp", ms, 68, E, np.array_equal(I32[:S].cpu().numpy(), orc.cmp(a[:S], b[:S], S)))
     ms = timed(lambda: xmp.check(L.xmpIntegersPopcAsync(h.h, I32.data_ptr(), A.x, E)))
-    row("popc", ms, 36, E, np.array_equal(I32[:S].cpu().numpy().view(np.uint32), orc.popc(a[:S], S)))
+    row("popc", ms, 36, E, np.array_equal(I32[:S].cpu().numpy().view(np.uint32), orc.popc(a[:S], S)),
+        vs_copy=True)
     # add through index arrays (random permutations gathering a and b, scattering c): 96 B of
     # operands plus three 4-byte indices per op
     perms = [np.random.default_rng(60 + k).permutation(E).astype(np.uint32) for k in range(3)]
@@ -871,6 +911,45 @@ def run_elementwise(args):
     h.destroy()
 
 
+def run_crt(args):
+    """CRT-RSA private operations (RSA-2048: 1024-bit primes from GMP nextprime on seeded starts,
+    e = 65537, messages uniform below n): --count decryptions under --crt-keys keys through the
+    fused xmpIntegersPowmCRT, every result checked against its message."""
+    import torch
+    import oracle as orc
+    import xmp_b200 as xmp
+    torch.cuda.set_device(0)
+    count, nkeys = args.count, args.crt_keys
+    keys = _crt_keys(nkeys, 1024, 777)
+    rng = np.random.default_rng(778)
+    msgs, cts = [], []
+    for i in range(count):
+        kk = keys[i % nkeys]
+        nn = orc.to_int(kk["n"])
+        mm = int.from_bytes(rng.bytes(256), "little") % nn
+        msgs.append(mm)
+        cts.append(pow(mm, 65537, nn))
+    h = xmp.Handle()
+    stream = torch.cuda.current_stream()
+    h.set_stream(stream.cuda_stream)
+    C = h.integers(2048, count, np.stack([orc.from_int(c, 64) for c in cts]))
+    ka = {f: h.integers(1024, nkeys, np.stack([kk[f] for kk in keys])) for f in ("p", "q", "dp", "dq", "qinv")}
+    out = h.integers(2048, count)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device="cuda")
+    step = lambda: xmp.powm_crt(h, out, C, ka["p"], ka["q"], ka["dp"], ka["dq"], ka["qinv"], count, asynchronous=True)
+    ms = statistics.median(_timed_events(step, stream, flush, args.steps, args.warmup))
+    ok = [orc.to_int(r) for r in out.export()] == msgs
+    line = {"metric": "CRT-RSA-2048 private operations/s (fused kernel)", "value": count / (ms * 1e-3),
+            "unit": "ops/s", "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "dtype": "u32", "data": "synthetic (seeded keys and messages)",
+            "config": {"workload": "RSA-2048 decryption by CRT x %d, %d keys" % (count, nkeys)},
+            "result_check": ok}
+    print(json.dumps(line), flush=True)
+    for v in [C, out] + list(ka.values()):
+        v.destroy()
+    h.destroy()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -885,7 +964,7 @@ def main():
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="headline workload only (no config 1/2/3 or reference GPU)")
     ap.add_argument("--force-config", default=None, help="lanes,limbs,window: time this powm kernel configuration")
-    ap.add_argument("--workload", default="powm2048", choices=["powm2048", "mixed", "serve", "elementwise"])
+    ap.add_argument("--workload", default="powm2048", choices=["powm2048", "mixed", "serve", "elementwise", "crt"])
     ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--serve-peak-requests", type=int, default=3000)
     ap.add_argument("--serve-sync-requests", type=int, default=40)
@@ -900,6 +979,9 @@ def main():
         return
     if args.workload == "elementwise":
         run_elementwise(args)
+        return
+    if args.workload == "crt":
+        run_crt(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

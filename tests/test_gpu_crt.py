@@ -20,10 +20,10 @@ def _decrypt(h, keys, cts, half_bits, dexp_bits=None):
     hn = half_bits // 32
     count, nkeys = len(cts), len(keys)
     rows = {k: np.stack([kk[k] for kk in keys]) for k in ("p", "q", "dp", "dq", "qinv")}
-    if dexp_bits:  # the same exponents held in arrays of another precision
-        for k in ("dp", "dq"):
-            r = np.zeros((nkeys, dexp_bits // 32), dtype=np.uint32)
-            w = min(hn, dexp_bits // 32)
+    if dexp_bits:  # the same exponents held in arrays of another precision (one for both, or (dp, dq))
+        for k, bits in zip(("dp", "dq"), dexp_bits if isinstance(dexp_bits, tuple) else (dexp_bits, dexp_bits)):
+            r = np.zeros((nkeys, bits // 32), dtype=np.uint32)
+            w = min(hn, bits // 32)
             r[:, :w] = rows[k][:, :w]
             rows[k] = r
     C = h.integers(2 * half_bits, count, np.stack([oracle.from_int(c, 2 * hn) for c in cts]))
@@ -80,6 +80,22 @@ def test_crt_toy_key_and_exponent_precision(handle):
     cts = [pow(m, 65537, n) for m in msgs]
     assert _decrypt(handle, [key], cts, 64) == msgs
     assert _decrypt(handle, [key], cts, 64, dexp_bits=128) == msgs
+    # dp and dq in arrays of different precisions: both halves of an operation scan the wider one
+    assert _decrypt(handle, [key], cts, 64, dexp_bits=(32, 128)) == msgs
+    assert _decrypt(handle, [key], cts, 64, dexp_bits=(96, 32)) == msgs
+
+
+def test_crt_mixed_exponent_precisions_full_size_key(handle):
+    """1024-bit halves with dq held in a 2048-bit array and dp in its own 1024-bit one."""
+    keys = _keys(3, 1024, 4200)
+    rng = np.random.default_rng(4201)
+    msgs, cts = [], []
+    for i in range(200):
+        n = oracle.to_int(keys[i % 3]["n"])
+        m = int.from_bytes(rng.bytes(256), "little") % n
+        msgs.append(m)
+        cts.append(pow(m, 65537, n))
+    assert _decrypt(handle, keys, cts, 1024, dexp_bits=(1024, 2048)) == msgs
 
 
 def test_crt_errors(handle):

@@ -233,3 +233,54 @@ def test_powm_bench_workload_sample(handle):
     sample = np.arange(0, count, 997)
     want, _ = oracle.powm(x[sample], e[sample], m[sample], len(sample))
     assert np.array_equal(got[sample], want)
+
+
+@pytest.mark.parametrize("lanes,limbs", [(4, 4), (4, 8), (4, 12), (4, 16), (1, 1), (1, 2), (1, 5), (1, 8),
+                                         (1, 12), (1, 16)])
+def test_powm_squaring_shapes(handle, lanes, limbs):
+    """The shapes whose squarings use the specialised product (four-lane blocks fed into the reduction,
+    per-thread separated scanning), at several windows, with full-length moduli, moduli whose top limbs
+    are zero, bases 0, 1 and m - 1 and all-ones exponents."""
+    bits = lanes * limbs * 32
+    n = bits // 32
+    count = 320
+    m = oracle.full_length_odd(900 + bits, count, n)
+    m[1::4, n // 2:] = 0  # a quarter of the moduli with their top half zero
+    m[1::4, max(0, n // 2 - 1)] |= np.uint32(1 << 31) if n > 1 else np.uint32(0)
+    m[:, 0] |= np.uint32(1)
+    x = oracle.below(901 + bits, m)
+    x[2::16] = 0
+    x[3::16] = 0
+    x[3::16, 0] = 1
+    x[5::16] = m[5::16]
+    x[5::16, 0] -= np.uint32(1)
+    e = oracle.random_limbs(902 + bits, count, n)
+    e[7::16] = 0xFFFFFFFF
+    want, _ = oracle.powm(x, e, m, count)
+    X, E, M = (handle.integers(bits, count, v) for v in (x, e, m))
+    O = handle.integers(bits, count)
+    try:
+        for w in (1, 3, 6):
+            xmp.powm_with_config(handle, O, X, E, M, count, xmp.PowmConfig(0, lanes, limbs, w))
+            got = O.export()
+            bad = np.nonzero(~np.all(got == want, axis=1))[0]
+            assert len(bad) == 0, "window %d: mismatch at %s" % (w, bad[:8])
+    finally:
+        for v in (X, E, M, O):
+            v.destroy()
+
+
+@pytest.mark.parametrize("bits,alg", [(12288, xmp.ALG_DEFAULT), (16384, xmp.ALG_DEFAULT),
+                                      (16384, xmp.ALG_DIGITMP), (20480, xmp.ALG_DEFAULT),
+                                      (32768, xmp.ALG_DEFAULT)])
+def test_powm_beyond_8192_bits(handle, bits, alg):
+    """Above the reference's largest tuned precision (8192 bits, src/powm.cu:61): the register kernels
+    up to 16,384 bits (32 lanes x 12 / 16 limbs) and the digit-serial kernel beyond, which the
+    reference also uses past its tables (src/powm.cu:197-208).  Short exponents keep GMP fast."""
+    count = 8
+    x, e, m = _case(400 + bits // 32, count, bits)
+    e = e[:, :2].copy()
+    e[0] = 0
+    e[1, 1] = 0xFFFFFFFF
+    want, _ = oracle.powm(x, e, m, count)
+    assert np.array_equal(_run(handle, x, e, m, count, alg), want)

@@ -257,7 +257,9 @@ xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t h, const xmpPowmBatchItem_t
   for (auto &b : p->bins) {
     if (b.serial) continue;
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, b.k->batch_fn, 128, 0);
+    if (b.k->smem > 48 * 1024)
+      cudaFuncSetAttribute(b.k->batch_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b.k->smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, b.k->batch_fn, 128, b.k->smem);
     occ = std::max(occ, 1);
     const uint32_t per_item = 32 / b.cfg.tpi;
     uint64_t items = 0;
@@ -276,13 +278,10 @@ xmpError_t XMPAPI xmpPowmBatchPlanCreate(xmpHandle_t h, const xmpPowmBatchItem_t
   }
   // CRT items: window tables for all instances at once, or chunks of what half the scratch limit holds
   for (auto &c : p->crt) {
-    const size_t per_inst = (size_t)c.cfg.tpi * c.cfg.limbs * ((size_t)1 << c.cfg.window) * 4;
-    const uint32_t per_block = 128 / c.cfg.tpi;
-    while (c.cfg.window > 1 && per_inst * per_block > scratch_limit(h) / 2) c.cfg.window--;
-    const size_t per = (size_t)c.cfg.tpi * c.cfg.limbs * ((size_t)1 << c.cfg.window) * 4;
-    uint64_t fit = (scratch_limit(h) / 2) / per / per_block * per_block;
-    if (fit < per_block) return fail(xmpErrorIncreaseScratchLimit);
-    c.chunk = (uint32_t)std::min<uint64_t>(c.item.count, fit);
+    while ((c.chunk = crt_chunk_for(c.cfg, scratch_limit(h) / 2, c.item.count)) == 0) {
+      if (c.cfg.window <= 1) return fail(xmpErrorIncreaseScratchLimit);
+      c.cfg.window--;
+    }
     c.table_offset = bytes;
     bytes += crt_table_bytes(c.cfg, c.chunk);
     bytes = (bytes + 255) & ~(size_t)255;

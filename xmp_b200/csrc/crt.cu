@@ -15,7 +15,9 @@ std::vector<CrtKernelEntry> &crt_registry() {
 
 #define XMPB_REGISTER_CRT(TPI, L)                                                                 \
   static void crt_launch_##TPI##_##L(const CrtArgs &a, int grid, cudaStream_t s) {               \
-    crt_kernel<TPI, L><<<grid, 128, 0, s>>>(a);                                                   \
+    static bool attr = false;                                                                     \
+    powm_smem_attr(crt_kernel<TPI, L>, powm_smem_bytes(TPI, L), attr);                            \
+    crt_kernel<TPI, L><<<grid, 128, powm_smem_bytes(TPI, L), s>>>(a);                             \
   }                                                                                               \
   static CrtKernelRegistrar crt_reg_##TPI##_##L(TPI, L, crt_launch_##TPI##_##L);
 
@@ -47,7 +49,7 @@ CrtConfig crt_config(uint32_t nlimbs, uint32_t exp_bits, uint32_t count, uint32_
     // the powm heuristic's cost model: padding squared, lane overhead, starved SMs below 4 warps each
     const double pad = (double)cap / nlimbs;
     const double work = pad * pad * (4.0 * e.limbs + 12.0) / (4.0 * e.limbs);
-    const double threads = (double)count * e.tpi;
+    const double threads = (double)count * e.tpi * 2;  // a pair of groups per instance
     const double starve = threads < want_threads ? want_threads / threads : 1.0;
     const double score = work * starve;
     if (score < best_score) {
@@ -62,15 +64,22 @@ CrtConfig crt_config(uint32_t nlimbs, uint32_t exp_bits, uint32_t count, uint32_
 }
 
 size_t crt_table_bytes(const CrtConfig &c, uint32_t count) {
-  const size_t threads = round_up((uint32_t)std::min<uint64_t>((uint64_t)count * c.tpi, 0xffffff80ull), 128);
+  const size_t threads = round_up((uint32_t)std::min<uint64_t>((uint64_t)count * c.tpi * 2, 0xffffff80ull), 128);
   return threads * (size_t)c.limbs * ((size_t)1 << c.window) * 4;
+}
+
+uint32_t crt_chunk_for(const CrtConfig &c, size_t limit, uint32_t count) {
+  const uint32_t per_block = 128 / (2 * c.tpi);  // a pair of groups per instance
+  const size_t per_inst = (size_t)2 * c.tpi * c.limbs * ((size_t)1 << c.window) * 4;
+  const uint64_t fit = std::min<uint64_t>(limit / per_inst, (1ull << 31) / (2 * c.tpi)) / per_block * per_block;
+  return fit < per_block ? 0u : (uint32_t)std::min<uint64_t>(count, fit);
 }
 
 void crt_launch(const CrtConfig &c, CrtArgs a, uint32_t count, uint32_t chunk, cudaStream_t s) {
   for (uint32_t start = 0; start < count; start += chunk) {
     a.start = start;
     a.count = std::min(chunk, count - start);
-    c.launch(a, grid_for((uint64_t)a.count * c.tpi, 128), s);
+    c.launch(a, grid_for((uint64_t)a.count * c.tpi * 2, 128), s);
   }
 }
 
@@ -120,15 +129,8 @@ xmpError_t XMPAPI xmpIntegersPowmCRTAsync(xmpHandle_t h, xmpIntegers_t out, cons
   if (!cfg.launch) return xmpErrorUnsupported;
   // chunk so the window tables fit the scratch limit; shrink the window when one block does not fit
   const size_t limit = scratch_limit(h);
-  const uint32_t per_block = 128 / cfg.tpi;
-  uint32_t chunk = count;
-  while (true) {
-    const size_t per_inst = (size_t)cfg.tpi * cfg.limbs * ((size_t)1 << cfg.window) * 4;
-    uint64_t fit = limit / per_inst / per_block * per_block;
-    if (fit >= per_block) {
-      chunk = (uint32_t)std::min<uint64_t>(count, fit);
-      break;
-    }
+  uint32_t chunk;
+  while ((chunk = crt_chunk_for(cfg, limit, count)) == 0) {
     if (cfg.window <= 1) return xmpErrorIncreaseScratchLimit;
     cfg.window--;
   }

@@ -30,6 +30,9 @@ struct CrtConfig {
 CrtConfig crt_config(uint32_t nlimbs, uint32_t exp_bits, uint32_t count, uint32_t sm_count);
 // Scratch bytes of the window tables of one launch of `count` instances.
 size_t crt_table_bytes(const CrtConfig &c, uint32_t count);
+// Instances per launch whose window tables fit `limit` bytes, in whole CTAs and at most `count`
+// (0: not even one CTA fits).  Capped so that a launch's thread index stays below 2^31.
+uint32_t crt_chunk_for(const CrtConfig &c, size_t limit, uint32_t count);
 // Launches `count` instances in chunks of at most `chunk` (a.table sized for one chunk).
 void crt_launch(const CrtConfig &c, CrtArgs a, uint32_t count, uint32_t chunk, cudaStream_t s);
 xmpError_t crt_validate(xmpHandle_t h, xmpIntegers_t out, xmpIntegers_t c, xmpIntegers_t p, xmpIntegers_t q,

@@ -27,6 +27,8 @@ struct PowmKernelEntry {
   PowmBatchLauncher launch_batch;
   const void *batch_fn;
   PowmLauncher launch_r2;
+  PowmLauncher launch_ct;  // constant schedule (fixed window over the exponent precision), for secret exponents
+  uint32_t smem;           // dynamic shared memory per 128-thread CTA (the four-lane squaring's blocks)
 };
 
 std::vector<PowmKernelEntry> &powm_registry();
@@ -34,26 +36,45 @@ const PowmKernelEntry *powm_find(int tpi, int limbs);
 
 struct PowmKernelRegistrar {
   PowmKernelRegistrar(int tpi, int limbs, PowmLauncher l, const void *fn, PowmBatchLauncher lb, const void *bfn,
-                      PowmLauncher lr2) {
-    powm_registry().push_back(PowmKernelEntry{tpi, limbs, l, fn, lb, bfn, lr2});
+                      PowmLauncher lr2, PowmLauncher lct, uint32_t smem) {
+    powm_registry().push_back(PowmKernelEntry{tpi, limbs, l, fn, lb, bfn, lr2, lct, smem});
   }
 };
 
+// Raises a kernel's dynamic shared memory limit above the 48 KB default once (needs a current device).
+template <class F>
+inline void powm_smem_attr(F *fn, uint32_t bytes, bool &done) {
+  if (!done && bytes > 48 * 1024) {
+    cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    done = true;
+  }
+}
+
 #define XMPB_REGISTER_POWM(TPI, L)                                                                   \
   static void powm_launch_##TPI##_##L(const PowmArgs &a, int grid, cudaStream_t s) {                \
-    powm_kernel<TPI, L><<<grid, 128, 0, s>>>(a);                                                     \
+    static bool attr = false;                                                                         \
+    powm_smem_attr(powm_kernel<TPI, L>, powm_smem_bytes(TPI, L), attr);                              \
+    powm_kernel<TPI, L><<<grid, 128, powm_smem_bytes(TPI, L), s>>>(a);                              \
   }                                                                                                   \
   static void powm_launch_batch_##TPI##_##L(const PowmBatchArgs &a, int grid, cudaStream_t s) {     \
-    powm_batch_kernel<TPI, L><<<grid, 128, 0, s>>>(a);                                               \
+    static bool attr = false;                                                                         \
+    powm_smem_attr(powm_batch_kernel<TPI, L>, powm_smem_bytes(TPI, L), attr);                        \
+    powm_batch_kernel<TPI, L><<<grid, 128, powm_smem_bytes(TPI, L), s>>>(a);                        \
   }                                                                                                   \
   static void powm_launch_r2_##TPI##_##L(const PowmArgs &a, int grid, cudaStream_t s) {             \
     r2_kernel<TPI, L><<<grid, 128, 0, s>>>(a);                                                       \
+  }                                                                                                   \
+  static void powm_launch_ct_##TPI##_##L(const PowmArgs &a, int grid, cudaStream_t s) {             \
+    static bool attr = false;                                                                         \
+    powm_smem_attr(powm_kernel<TPI, L, true>, powm_smem_bytes(TPI, L), attr);                        \
+    powm_kernel<TPI, L, true><<<grid, 128, powm_smem_bytes(TPI, L), s>>>(a);                        \
   }                                                                                                   \
   static PowmKernelRegistrar powm_reg_##TPI##_##L(TPI, L, powm_launch_##TPI##_##L,                  \
                                                   (const void *)powm_kernel<TPI, L>,                 \
                                                   powm_launch_batch_##TPI##_##L,                     \
                                                   (const void *)powm_batch_kernel<TPI, L>,           \
-                                                  powm_launch_r2_##TPI##_##L);
+                                                  powm_launch_r2_##TPI##_##L, powm_launch_ct_##TPI##_##L, \
+                                                  powm_smem_bytes(TPI, L));
 
 // Window bits for a k-bit exponent.  Sliding window (register kernels with
 // powm_sliding): minimises the table build (2^(W-1) multiplies, weighted 5/4)

@@ -40,6 +40,7 @@
 #pragma once
 #include "internal.h"
 #include "mont.cuh"
+#include "sqr.cuh"
 
 namespace xmpb {
 
@@ -67,12 +68,13 @@ struct PowmArgs {
 // is worse there) and at small precisions, where the control is a larger
 // share of a step.
 __host__ __device__ constexpr bool powm_sliding(int TPI, int L) {
-  return (TPI == 1 && (L == 24 || L == 32)) ||
+  return !powm_sqr(TPI, L) && (
+         (TPI == 1 && (L == 24 || L == 32)) ||
          (TPI == 2 && (L == 8 || L == 16)) ||
          (TPI == 4 && (L == 5 || L == 6 || L == 16)) ||
          (TPI == 8 && (L == 4 || L == 5 || L == 6 || L == 16)) ||
          (TPI == 16 && (L == 2 || L == 4 || L == 6 || L == 16)) ||
-         (TPI == 32 && (L == 8 || L == 16));
+         (TPI == 32 && (L == 8 || L == 16)));
 }
 
 // Window-table entries for window bits W.  Sliding: slot 0 holds Mont(1) and
@@ -244,9 +246,13 @@ __device__ __forceinline__ uint32_t exp_bitlen(const Group<TPI> &G, const ArrayV
 // One instance group: op instance i of `args` (every lane of the warp calls
 // this together; `valid` lanes store their result).  `slot` is this lane's
 // window-table slot (entry e at slot + e*32*L).
-template <int TPI, int L>
+// CT (constant schedule, for secret exponents): the fixed window over the
+// exponent's whole precision for every shape -- the same sequence of
+// squarings and multiplies whatever the exponent bits, as the reference's fwe
+// scans them (powm/powm.h:39-127); the table is the fixed-window table.
+template <int TPI, int L, bool CT = false>
 __device__ __forceinline__ void powm_instance(const Group<TPI> &G, const PowmArgs &args, uint32_t i, bool valid,
-                                              uint32_t *slot) {
+                                              uint32_t *slot, const SqrSmem &sm) {
   const uint32_t eb = in_element(args.base, i), ee = in_element(args.exp, i), em = in_element(args.mod, i);
 
   uint32_t n[L];
@@ -254,13 +260,16 @@ __device__ __forceinline__ void powm_instance(const Group<TPI> &G, const PowmArg
   const uint32_t np0 = neg_inv32(G.bcast(n[0], 0));
 
   const uint32_t W = args.window;
-  constexpr bool kSliding = powm_sliding(TPI, L);
+  constexpr bool kSliding = powm_sliding(TPI, L) && !CT;
   // sliding: from this instance's own top bit (its lanes agree), instances of a warp scan independently;
-  // fixed: from the highest window any instance of the warp needs (warp-uniform)
+  // fixed: from the highest window any instance of the warp needs (warp-uniform); CT: from the top of
+  // the exponent's precision
   ExpCursor cur;
   uint32_t nwin = 0;
   if constexpr (kSliding) {
     cursor_init(cur, args.exp, ee, (int32_t)exp_bitlen<TPI>(G, args.exp, ee) - 1);
+  } else if constexpr (CT) {
+    nwin = (args.exp.nlimbs * 32 + W - 1) / W;
   } else {
     uint32_t ebits = exp_bitlen<TPI>(G, args.exp, ee);
     ebits = __reduce_max_sync(kFull, ebits);
@@ -347,22 +356,37 @@ __device__ __forceinline__ void powm_instance(const Group<TPI> &G, const PowmArg
     }
 
     // W squarings and one table multiply per window (window value 0 multiplies
-    // by Mont(1)); the window's entry is loaded before its squarings.
+    // by Mont(1)); the window's entry is loaded before its squarings, or, where
+    // the shape squares with the specialised product, after them.
     uint32_t win = exp_window(args.exp, ee, (nwin - 1) * W, W);
     slot_load<L>(slot + win * entry_stride, acc);
 #pragma unroll 1
     for (int32_t wi = (int32_t)nwin - 2; wi >= 0; wi--) {
       win = exp_window(args.exp, ee, (uint32_t)wi * W, W);
-      uint32_t y[L];
-      slot_load<L>(slot + win * entry_stride, y);
+      if constexpr (powm_sqr(TPI, L)) {
 #pragma unroll 1
-      for (uint32_t s = 0; s <= W; s++) {
-        uint32_t bsel[L];
+        for (uint32_t s = 0; s < W; s++) {
+          mont_square<TPI, L>(G, x, acc, n, np0, sm);
 #pragma unroll
-        for (int k = 0; k < L; k++) bsel[k] = (s < W) ? acc[k] : y[k];
-        mont_mul<TPI, L>(G, x, acc, bsel, n, np0);
+          for (int k = 0; k < L; k++) acc[k] = x[k];
+        }
+        uint32_t y[L];
+        slot_load<L>(slot + win * entry_stride, y);
+        mont_mul<TPI, L>(G, x, acc, y, n, np0);
 #pragma unroll
         for (int k = 0; k < L; k++) acc[k] = x[k];
+      } else {
+        uint32_t y[L];
+        slot_load<L>(slot + win * entry_stride, y);
+#pragma unroll 1
+        for (uint32_t s = 0; s <= W; s++) {
+          uint32_t bsel[L];
+#pragma unroll
+          for (int k = 0; k < L; k++) bsel[k] = (s < W) ? acc[k] : y[k];
+          mont_mul<TPI, L>(G, x, acc, bsel, n, np0);
+#pragma unroll
+          for (int k = 0; k < L; k++) acc[k] = x[k];
+        }
       }
     }
   }
@@ -386,19 +410,36 @@ __device__ __forceinline__ void powm_instance(const Group<TPI> &G, const PowmArg
 // kernel needs 96 (5 CTAs/SM).  The one-shot kernel keeps the allocator's own
 // choice (a bound equal to its natural count still changed its schedule and
 // cost 2.4% at 2048 bits).
-constexpr int powm_batch_min_blocks(int L) { return (L > 8 && L <= 12) ? 5 : 1; }
+constexpr int powm_batch_min_blocks(int TPI, int L) {
+  return (L > 8 && L <= 12) ? 5 : (TPI == 4 && L == 8) ? 4 : 1;  // 4 x 8: the squaring's state took 140
+}
 
+// The four-lane squaring's blocks (sqr.cuh) live in the kernel's dynamic shared memory.
 template <int TPI, int L>
+__device__ __forceinline__ SqrSmem powm_smem_setup() {
+  extern __shared__ uint4 powm_dyn_smem[];
+  SqrSmem sm{};
+  if constexpr (powm_smem_bytes(TPI, L) > 0) {
+    sm = sqr_smem<TPI, L>(powm_dyn_smem, threadIdx.x % TPI);
+    sqr_smem_init<L>(sm);
+    __syncthreads();
+  }
+  return sm;
+}
+
+template <int TPI, int L, bool CT = false>
 __global__ void __launch_bounds__(128) powm_kernel(PowmArgs args) {
+  const SqrSmem sm = powm_smem_setup<TPI, L>();
   Group<TPI> G;
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t local = gtid / TPI;
   const bool valid = local < args.count;
   // Lanes past the end run a copy of the last instance so every shfl sees a full warp.
   const uint32_t i = args.start + (valid ? local : args.count - 1);
-  uint32_t *slot = args.table + (size_t)(gtid >> 5) * ((size_t)32 * L * powm_table_entries(args.window, powm_sliding(TPI, L))) +
+  uint32_t *slot = args.table +
+                   (size_t)(gtid >> 5) * ((size_t)32 * L * powm_table_entries(args.window, powm_sliding(TPI, L) && !CT)) +
                    (size_t)(threadIdx.x & 31) * L;
-  powm_instance<TPI, L>(G, args, i, valid, slot);
+  powm_instance<TPI, L, CT>(G, args, i, valid, slot, sm);
 }
 
 // R^2 mod N (R = 2^(32 * TPI * L)) for elements start .. start+count-1 of
@@ -439,7 +480,8 @@ struct PowmBatchArgs {
 };
 
 template <int TPI, int L>
-__global__ void __launch_bounds__(128, powm_batch_min_blocks(L)) powm_batch_kernel(PowmBatchArgs b) {
+__global__ void __launch_bounds__(128, powm_batch_min_blocks(TPI, L)) powm_batch_kernel(PowmBatchArgs b) {
+  const SqrSmem sm = powm_smem_setup<TPI, L>();
   Group<TPI> G;
   const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   uint32_t *slot = b.table + (size_t)gwarp * ((size_t)32 * L * powm_table_entries(b.window, powm_sliding(TPI, L))) +
@@ -458,7 +500,7 @@ __global__ void __launch_bounds__(128, powm_batch_min_blocks(L)) powm_batch_kern
     const uint32_t i = a.start + (valid ? local : a.count - 1);
     PowmArgs args = a;
     args.window = b.window;
-    powm_instance<TPI, L>(G, args, i, valid, slot);
+    powm_instance<TPI, L>(G, args, i, valid, slot, sm);
   }
 }
 

@@ -10,7 +10,10 @@
 // pinned staging, one copy moves them to the device, a staging kernel
 // interleaves them into a contiguous range of op slots, the powm kernel runs
 // on those slots with the key's constants gathered through a per-slot key
-// index, and the results come back with one copy.  Waves go out on a pool of
+// index, and the results come back with one copy.  Request exponents are
+// treated as secret: the kernel is the constant-schedule form (a fixed window
+// over the exponent's whole precision, the same multiplications for every
+// exponent value).  Waves go out on a pool of
 // streams, so requests that arrive while others are on the GPU start as soon
 // as slots are free and run alongside them.  The slot rings (one per class,
 // sized from the HBM budget) are the admission control: a request waits on
@@ -213,10 +216,9 @@ static void choose_configs(xmpServer_t s, Class &c) {
     PowmConfig cfg;
     bool ok = tuner_lookup_powm(s->h, c.n, c.precision, ops, &cfg) && cfg.dist == kDistLanes &&
               (uint32_t)(cfg.tpi * cfg.limbs) == c.cap && powm_find(cfg.tpi, cfg.limbs);
-    if (!ok) {
-      cfg = powm_default_config(c.n, c.precision, ops, xmpAlgorithmDefault, s->h->sm_count, c.cap);
-      cfg.window = window_for_bits(c.precision, powm_sliding(cfg.tpi, cfg.limbs));
-    }
+    if (!ok) cfg = powm_default_config(c.n, c.precision, ops, xmpAlgorithmDefault, s->h->sm_count, c.cap);
+    // requests carry private exponents: the constant-schedule kernel, fixed window over the full precision
+    cfg.window = window_for_bits(c.precision, false);
     c.cfg[b] = cfg;
     c.entry[b] = powm_find(cfg.tpi, cfg.limbs);
   }
@@ -286,7 +288,7 @@ static bool launch_wave(xmpServer_t s, Class &c, Wave *w, uint32_t load) {
   a.count = w->ops;
   a.window = cfg.window;
   a.table = c.table + (size_t)w->first * c.table_words;
-  c.entry[b]->launch(a, grid_for((uint64_t)w->ops * cfg.tpi, 128), st);
+  c.entry[b]->launch_ct(a, grid_for((uint64_t)w->ops * cfg.tpi, 128), st);
   slots_to_rows<<<dim3(div_up(w->ops, 128), c.ngroups), 128, 0, st>>>(c.slot_out, n, c.slots, w->first,
                                                                          c.rows_out + off, w->ops);
   if (cudaMemcpyAsync(c.pin_out + off, c.rows_out + off, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
@@ -517,7 +519,7 @@ xmpError_t XMPAPI xmpServerCreate(xmpHandle_t h, const uint32_t *precisions, uin
     size_t tw = 0;
     for (int b = 0; b < kBuckets; b++) {
       if (!c.entry[b]) return fail(xmpErrorUnsupported);
-      tw = std::max(tw, (size_t)cap * powm_table_entries(c.cfg[b].window, powm_sliding(c.cfg[b].tpi, c.cfg[b].limbs)));
+      tw = std::max(tw, (size_t)cap * powm_table_entries(c.cfg[b].window, false));
     }
     c.table_words = tw;
     c.kcap = round_up(cf.max_keys, 32);
