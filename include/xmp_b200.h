@@ -19,8 +19,13 @@ extern "C" {
 /* One powm kernel configuration.
  *   distribution: 0 = register kernel with `lanes` threads per instance and
  *                 `limbs` 32-bit limbs per thread (lanes = 1 is the per-thread
- *                 distribution), 1 = digit-serial (lanes/limbs ignored);
- *   window:       fixed-window exponent bits, 1..7. */
+ *                 distribution), 1 = digit-serial (lanes/limbs ignored),
+ *                 2 = one instance per CTA (moduli up to 4096 bits; the library
+ *                 sets limbs to the CTA's operand size, 32/64/96/128, and
+ *                 ignores lanes) -- the lowest latency for a small batch, and
+ *                 the default choice for batches of up to one (1024-bit and
+ *                 smaller moduli) or two (larger) instances per SM;
+ *   window:       exponent window bits, 1..7. */
 typedef struct {
   int32_t distribution;
   int32_t lanes;

@@ -292,18 +292,26 @@ def test_error_codes(handle):
         big.destroy()
     finally:
         handle.set_policy(None)
-    # scratch limit too small for any window table (import first: it stages host data through scratch)
-    x = handle.integers(1024, 64, oracle.full_length_odd(1, 64, 32))
+    # scratch limit too small for any window table (import first: it stages host data through scratch);
+    # 1,024 instances go to the lane kernels, whose tables live in scratch
+    x = handle.integers(1024, 1024, oracle.full_length_odd(1, 1024, 32))
+    ym = oracle.full_length_odd(2, 16, 32)
+    y, yo = handle.integers(1024, 16, ym), handle.integers(1024, 16)
     tiny = handle.policy()
     tiny.set_scratch_limit(64)
     handle.set_policy(tiny)
     try:
         with pytest.raises(xmp.XmpError) as e:
-            xmp.powm(handle, x, x, x, x, 64)
+            xmp.powm(handle, x, x, x, x, 1024)
         assert e.value.code == xmp.ERR["xmpErrorIncreaseScratchLimit"]
-        x.destroy()
+        # a small batch runs one instance per CTA with its table in shared memory: no scratch needed
+        xmp.powm(handle, yo, y, y, y, 16)
     finally:
         handle.set_policy(None)
+    want, _ = oracle.powm(ym, ym, ym, 16)
+    assert np.array_equal(yo.export(), want)
+    for v in (x, y, yo):
+        v.destroy()
     dev = np.zeros(1, dtype=np.int32)
     import ctypes
     d = ctypes.c_int32(-1)

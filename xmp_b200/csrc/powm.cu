@@ -43,9 +43,22 @@ int window_for_bits(uint32_t exp_bits, bool sliding) {
   return best;
 }
 
+bool powm_cta_preferred(uint32_t nlimbs, uint32_t count, uint32_t sm_count) {
+  const uint32_t limbs = powm_cta_limbs(nlimbs);
+  if (!limbs) return false;
+  // A CTA per instance runs it at its lone latency while the SMs hold the batch; the lane kernels
+  // need thousands of instances before their throughput beats that.  Measured on B200 through
+  // xmpIntegersPowm (full-length exponents), CTA vs the fastest lane kernel at 1 / 148 / 296 / 444
+  // instances: 1024 bits 1.90/1.91/1.93/2.20 vs 2.13 ms; 2048 bits 5.08/5.12/6.42/11.2 vs 8.10 ms;
+  // 3072 bits 10.97/11.05/22.0 vs 15.9 ms; 4096 bits 25.3/25.6/51.2 vs 30.5 ms.  Up to 2048 bits
+  // two instances per SM fit (1024: 64 threads, 2048: 256 threads per CTA), above that one.
+  return count <= (limbs <= 64 ? 2u : 1u) * sm_count;
+}
+
 bool powm_config_valid(const PowmConfig &c, uint32_t nlimbs) {
   if (c.window < 1 || c.window > 7) return false;
   if (c.dist == kDistDigit) return true;
+  if (c.dist == kDistCta) return powm_cta_limbs(nlimbs) != 0 && (uint32_t)c.limbs == powm_cta_limbs(nlimbs);
   if ((uint64_t)c.tpi * c.limbs < nlimbs) return false;
   return powm_find(c.tpi, c.limbs) != nullptr;
 }
@@ -88,6 +101,7 @@ PowmConfig powm_default_config(uint32_t nlimbs, uint32_t exp_bits, uint32_t coun
 }
 
 size_t powm_table_bytes(const PowmConfig &cfg, uint32_t nlimbs, uint32_t count) {
+  if (cfg.dist == kDistCta) return 0;  // the table is in shared memory
   if (cfg.dist == kDistDigit) {
     // table + N, x, b, m, r, r2 working arrays, all nlimbs+2 words per instance
     size_t words = ((size_t)1 << cfg.window) * nlimbs + 6 * ((size_t)nlimbs + 2);
@@ -101,6 +115,19 @@ xmpError_t powm_run(xmpHandle_t h, const PowmConfig &cfg0, const OutView &out, c
                     const ArrayView &exp, const ArrayView &mod, uint32_t count) {
   PowmConfig cfg = cfg0;
   if (cfg.dist == kDistDigit) return powm_digit_run(h, cfg, out, base, exp, mod, count);
+  if (cfg.dist == kDistCta) {
+    PowmArgs a;
+    a.base = base;
+    a.exp = exp;
+    a.mod = mod;
+    a.out = out;
+    a.start = 0;
+    a.count = count;
+    a.window = cfg.window;
+    a.table = nullptr;
+    if (!powm_cta_launch((uint32_t)cfg.limbs, false, a, count, h->stream)) return xmpErrorUnsupported;
+    return check_cuda();
+  }
   const PowmKernelEntry *k = powm_find(cfg.tpi, cfg.limbs);
   if (!k) return xmpErrorUnsupported;
   size_t limit = scratch_limit(h);
@@ -138,6 +165,26 @@ xmpError_t powm_run(xmpHandle_t h, const PowmConfig &cfg0, const OutView &out, c
 
 }  // namespace xmpb
 
+// The configuration for a problem shape under the handle's policy (default algorithm): a choice set
+// for the exact shape, else one instance per CTA for small batches, else the selector, else the
+// heuristic.  An explicit algorithm takes the heuristic restricted to it.
+static PowmConfig powm_choose_config(xmpHandle_t h, uint32_t nlimbs, uint32_t exp_bits, uint32_t count) {
+  PowmConfig cfg;
+  const xmpAlgorithm_t alg = h->policy->algorithm;
+  int src = 0;
+  const bool tuned = (alg == xmpAlgorithmDefault) && tuner_lookup_powm(h, nlimbs, exp_bits, count, &cfg, &src);
+  if (tuned && src == 1) return cfg;
+  if (alg == xmpAlgorithmDefault && powm_cta_preferred(nlimbs, count, h->sm_count)) {
+    cfg = PowmConfig();
+    cfg.dist = kDistCta;
+    cfg.limbs = (int)powm_cta_limbs(nlimbs);
+    cfg.window = window_for_bits(exp_bits, true);
+    return cfg;
+  }
+  if (!tuned) cfg = powm_default_config(nlimbs, exp_bits, count, alg, h->sm_count);
+  return cfg;
+}
+
 static xmpError_t powm_entry(xmpHandle_t h, xmpIntegers_t out, xmpIntegers_t base, xmpIntegers_t exp,
                              xmpIntegers_t mod, uint32_t count, const PowmConfig *forced) {
   if (!h || !out || !base || !exp || !mod) return xmpErrorInvalidParameter;
@@ -154,10 +201,9 @@ static xmpError_t powm_entry(xmpHandle_t h, xmpIntegers_t out, xmpIntegers_t bas
   PowmConfig cfg;
   if (forced) {
     cfg = *forced;
+    if (cfg.dist == kDistCta) cfg.limbs = (int)powm_cta_limbs(mod->nlimbs);
   } else {
-    bool tuned = (p->algorithm == xmpAlgorithmDefault) &&
-                 tuner_lookup_powm(h, mod->nlimbs, exp->precision, count, &cfg);
-    if (!tuned) cfg = powm_default_config(mod->nlimbs, exp->precision, count, p->algorithm, h->sm_count);
+    cfg = powm_choose_config(h, mod->nlimbs, exp->precision, count);
   }
   if (!powm_config_valid(cfg, mod->nlimbs)) return xmpErrorUnsupported;
 
@@ -200,7 +246,7 @@ xmpError_t XMPAPI xmpIntegersPowmWithConfigAsync(xmpHandle_t h, xmpIntegers_t ou
   c.tpi = config->lanes;
   c.limbs = config->limbs;
   c.window = config->window;
-  if (c.dist != kDistLanes && c.dist != kDistDigit) return xmpErrorInvalidParameter;
+  if (c.dist != kDistLanes && c.dist != kDistDigit && c.dist != kDistCta) return xmpErrorInvalidParameter;
   return powm_entry(h, out, base, exp, mod, count, &c);
 }
 
@@ -221,10 +267,7 @@ xmpError_t XMPAPI xmpPowmGetConfig(xmpHandle_t h, uint32_t precision, uint32_t e
                                    xmpPowmConfig_t *config) {
   if (!h || !config || precision == 0 || precision % 32 || exp_precision == 0 || exp_precision % 32)
     return xmpErrorInvalidParameter;
-  PowmConfig c;
-  bool tuned = (h->policy->algorithm == xmpAlgorithmDefault) &&
-               tuner_lookup_powm(h, precision / 32, exp_precision, count, &c);
-  if (!tuned) c = powm_default_config(precision / 32, exp_precision, count, h->policy->algorithm, h->sm_count);
+  const PowmConfig c = powm_choose_config(h, precision / 32, exp_precision, count);
   config->distribution = c.dist;
   config->lanes = c.tpi;
   config->limbs = c.limbs;

@@ -7,14 +7,22 @@
 
 namespace xmpb {
 
-enum PowmDist : int { kDistLanes = 0, kDistDigit = 1 };
+enum PowmDist : int { kDistLanes = 0, kDistDigit = 1, kDistCta = 2 };
 
 struct PowmConfig {
-  int dist = kDistLanes;  // lanes: TPI x L register kernel; digit: digit-serial kernel
-  int tpi = 0;            // threads per instance (1 = per-thread)
-  int limbs = 0;          // limbs per lane
+  int dist = kDistLanes;  // lanes: TPI x L register kernel; digit: digit-serial kernel; cta: one instance per CTA
+  int tpi = 0;            // threads per instance (1 = per-thread; cta: 0)
+  int limbs = 0;          // limbs per lane (cta: limbs of the CTA's operands, 32 / 64 / 96 / 128)
   int window = 0;         // window bits
 };
+
+// CTA distribution (cta.cuh): operand size in limbs for an n-limb modulus (0: larger than 4096 bits).
+uint32_t powm_cta_limbs(uint32_t nlimbs);
+// Launches `count` instances from a.start, one CTA each (ct: the constant-schedule fixed window);
+// false if the size or window is not supported.  No scratch: the window table is in shared memory.
+bool powm_cta_launch(uint32_t limbs, bool ct, const PowmArgs &a, uint32_t count, cudaStream_t s);
+// Whether a batch this small runs faster one instance per CTA than on the lane kernels.
+bool powm_cta_preferred(uint32_t nlimbs, uint32_t count, uint32_t sm_count);
 
 typedef void (*PowmLauncher)(const PowmArgs &args, int grid, cudaStream_t stream);
 typedef void (*PowmBatchLauncher)(const PowmBatchArgs &args, int grid, cudaStream_t stream);
@@ -104,6 +112,8 @@ xmpError_t powm_digit_run(xmpHandle_t h, const PowmConfig &cfg, const OutView &o
                           const ArrayView &exp, const ArrayView &mod, uint32_t count);
 
 // Configuration chosen by the handle's tuner (selector / exhaustive table), if any.
-bool tuner_lookup_powm(xmpHandle_t h, uint32_t nlimbs, uint32_t exp_bits, uint32_t count, PowmConfig *cfg);
+// *source (optional): 1 = a choice set for the exact shape, 2 = the selector.
+bool tuner_lookup_powm(xmpHandle_t h, uint32_t nlimbs, uint32_t exp_bits, uint32_t count, PowmConfig *cfg,
+                       int *source = nullptr);
 
 }  // namespace xmpb

@@ -13,7 +13,9 @@
 // index, and the results come back with one copy.  Request exponents are
 // treated as secret: the kernel is the constant-schedule form (a fixed window
 // over the exponent's whole precision, the same multiplications for every
-// exponent value).  Waves go out on a pool of
+// exponent value).  While the GPU is nearly idle, small waves of up to 2048
+// bits run one op per CTA (cta.cuh); everything else runs on the lane
+// kernels.  Waves go out on a pool of
 // streams, so requests that arrive while others are on the GPU start as soon
 // as slots are free and run alongside them.  The slot rings (one per class,
 // sized from the HBM budget) are the admission control: a request waits on
@@ -123,6 +125,8 @@ struct Class {
   size_t table_words = 0;  // per slot
   PowmConfig cfg[kBuckets];
   const PowmKernelEntry *entry[kBuckets] = {};
+  bool cta[kBuckets] = {};  // waves of this size run one op per CTA (cta_limbs-limb operands)
+  uint32_t cta_limbs = 0;
   bool urgent = false;  // the largest precision: its waves bound the latency tail, so they get priority streams
   // scheduler-owned queues
   std::deque<Req *> pending;
@@ -221,6 +225,11 @@ static void choose_configs(xmpServer_t s, Class &c) {
     cfg.window = window_for_bits(c.precision, false);
     c.cfg[b] = cfg;
     c.entry[b] = powm_find(cfg.tpi, cfg.limbs);
+    // small waves on a quiet GPU: one op per CTA (its constant-schedule form), at a lone op's lowest
+    // latency -- only up to 2048 bits, where that form beats the lane kernels alone (one op: 5.8 vs
+    // 8.4 ms at 2048 bits; 3072 bits 15.1 vs 16.4, 4096 bits 31.6 vs 30.7 ms)
+    c.cta_limbs = powm_cta_limbs(c.n);
+    c.cta[b] = c.cta_limbs != 0 && c.cta_limbs <= 64 && ops <= s->h->sm_count;
   }
 }
 
@@ -241,7 +250,12 @@ static cudaEvent_t take_event(xmpServer_t s) {
   return e;
 }
 
-static bool launch_wave(xmpServer_t s, Class &c, Wave *w, uint32_t load) {
+// `load`: the class's ops in flight with this wave (picks the lane kernel's bucket); `gpu_load`: all
+// classes' ops in flight with this wave.  A wave runs one op per CTA only while the GPU is otherwise
+// nearly idle: CTAs of a lone op are fast but share SMs poorly (measured: with one op per CTA for
+// every wave of up to two ops per SM, a 70%-load mix of 2048-4096-bit requests had a 166 ms p99
+// against 58 ms on the lane kernels alone).
+static bool launch_wave(xmpServer_t s, Class &c, Wave *w, uint32_t load, uint32_t gpu_load) {
   const uint32_t n = c.n;
   const size_t row_bytes = (size_t)n * 4;
   for (size_t r = 0; r < w->reqs.size(); r++) {
@@ -288,7 +302,11 @@ static bool launch_wave(xmpServer_t s, Class &c, Wave *w, uint32_t load) {
   a.count = w->ops;
   a.window = cfg.window;
   a.table = c.table + (size_t)w->first * c.table_words;
-  c.entry[b]->launch_ct(a, grid_for((uint64_t)w->ops * cfg.tpi, 128), st);
+  if (c.cta[b] && gpu_load <= s->h->sm_count) {
+    if (!powm_cta_launch(c.cta_limbs, true, a, w->ops, st)) return false;
+  } else {
+    c.entry[b]->launch_ct(a, grid_for((uint64_t)w->ops * cfg.tpi, 128), st);
+  }
   slots_to_rows<<<dim3(div_up(w->ops, 128), c.ngroups), 128, 0, st>>>(c.slot_out, n, c.slots, w->first,
                                                                          c.rows_out + off, w->ops);
   if (cudaMemcpyAsync(c.pin_out + off, c.rows_out + off, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
@@ -387,9 +405,11 @@ static bool launch_ready(xmpServer_t s, bool *progress) {
       off += r->nops;
     }
     const uint32_t load = c.inflight_ops + take;
+    uint32_t gpu_load = take;
+    for (const auto &cc : s->classes) gpu_load += cc.inflight_ops;
     c.inflight.push_back(w);
     c.inflight_ops += take;
-    if (!launch_wave(s, c, w, load)) return false;
+    if (!launch_wave(s, c, w, load, gpu_load)) return false;
     idle--;
     *progress = true;
     std::lock_guard<std::mutex> lk(s->mu);

@@ -109,11 +109,13 @@ int tuner_lookup(xmpHandle_t h, int op, uint32_t bits, uint32_t exp_bits, uint32
 // with the same kernel -- and the window that minimises it
 // (window_for_bits, up to 7) beats the network's pick, whose fit does not
 // resolve the 1-2% between neighbouring windows.
-bool tuner_lookup_powm(xmpHandle_t h, uint32_t nlimbs, uint32_t exp_bits, uint32_t count, PowmConfig *cfg) {
+bool tuner_lookup_powm(xmpHandle_t h, uint32_t nlimbs, uint32_t exp_bits, uint32_t count, PowmConfig *cfg,
+                       int *source) {
   int src = 0;
   int slot = tuner_lookup(h, xmpTunePowm, nlimbs * 32, exp_bits, count, &src);
   if (slot < 0 || !powm_candidate(nlimbs, slot, cfg)) return false;
   if (src == 2) cfg->window = window_for_bits(exp_bits, cfg->dist != kDistDigit && powm_sliding(cfg->tpi, cfg->limbs));
+  if (source) *source = src;
   return true;
 }
 
