@@ -280,6 +280,47 @@ def config1_suite(h, stream, flush, steps, warmup, imad_peak, cpu_seconds):
             "result_check": ok}
 
 
+def latency_suite(h, stream, reps=5):
+    """One full-exponent modexp alone, per size, through xmpIntegersPowm: the library's default
+    choice for a batch of one (one instance per CTA) and the fastest lane kernel for it (the
+    warp-distributed heuristic), best of `reps` by CUDA events, both results checked against GMP."""
+    import torch
+    import oracle as orc
+    import xmp_b200 as xmp
+    out = {}
+    for bits in (1024, 2048, 3072, 4096):
+        x, e, m = make_inputs(bits, 1)
+        X, E, M, O = (h.integers(bits, 1) for _ in range(4))
+        for arr, rows in ((X, x), (E, e), (M, m)):
+            arr.import_(rows)
+        want, _ = orc.powm(x, e, m, 1)
+        res = {}
+        for name, alg in (("default", xmp.ALG_DEFAULT), ("lane_kernel", xmp.ALG_DISTRIBUTEDMP)):
+            pol = xmp.Policy(h)
+            pol.set_algorithm(alg)
+            h.set_policy(pol)
+            cfg = xmp.powm_get_config(h, bits, bits, 1)
+            fn = lambda: xmp.check(xmp.lib().xmpIntegersPowmAsync(h.h, O.x, X.x, E.x, M.x, 1), "xmpIntegersPowmAsync")
+            fn()
+            torch.cuda.synchronize()
+            ts = []
+            for _ in range(reps):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                fn()
+                b.record(stream)
+                torch.cuda.synchronize()
+                ts.append(a.elapsed_time(b))
+            h.set_policy(None)
+            pol.destroy()
+            res[name] = {"ms": min(ts), "distribution": cfg.distribution, "lanes": cfg.lanes, "limbs": cfg.limbs,
+                         "check": bool(np.array_equal(O.export(), want))}
+        out[str(bits)] = res
+        for v in (X, E, M, O):
+            v.destroy()
+    return out
+
+
 def reference_gpu_suite(stream, flush, steps, warmup, ours):
     """The reference XMP's own kernels on this GPU (oracle/_ref, built from its sources for
     sm_100a by oracle/build_ref.sh): modexp/s on the headline workload and the 1024-bit x 4,096
@@ -445,6 +486,7 @@ def run_ours(args, rank, world, local_rank):
         extra["config2_elementwise"] = {"ops": ew, "cpu_baseline_ops_per_s": ew_cpu, "hbm_peak_gbs": hbm,
                                         "imad_peak_timad_s": peaks["imad"]}
         extra["config3_mixed"] = mixed_suite(3, 1, 65536, 16384, 256)
+        extra["single_op_latency"] = latency_suite(h, stream)
         extra["seconds"] = time.perf_counter() - t0
 
     line = {

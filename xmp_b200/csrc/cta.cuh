@@ -139,17 +139,18 @@ __device__ __forceinline__ uint32_t cta_sub_if(CtaSmem<N> &s, uint32_t *r, const
 // carry into word n is c = hi(s_(n-1)) + (lo(s_(n-1)) != 0) and only the words
 // >= n - 1 of U are summed.  T's high half is therefore never resolved either:
 // its raw diagonal sums (dsumT) enter U's column sums directly; only T's low
-// half is resolved (it is m's operand).  A squaring forms the tiles on and
-// above the diagonal of the tile grid and counts the others twice.
+// half is resolved (it is m's operand).  (Squarings that form only the tiles
+// on and above the tile grid's diagonal, counting the others twice, measured
+// slower: one 2048-bit exponentiation 4.76 against 4.42 ms -- the tile phase
+// does not get shorter and the diagonal sums pay for the extra predicates.)
 enum CtaCols : int { kColsFull = 0, kColsLow = 1, kColsHigh = 2 };
 
-template <int N, int MODE, bool SQR>
+template <int N, int MODE>
 __device__ __forceinline__ void cta_cols(CtaSmem<N> &s, const uint32_t *x, const uint32_t *y,
                                          unsigned long long *out) {
   using C = CtaShape<N>;
   const int tid = threadIdx.x, ti = tid / C::Q, tj = tid % C::Q;
-  const bool need = (MODE == kColsLow ? ti + tj < C::Q : MODE == kColsHigh ? ti + tj >= C::Q - 2 : true) &&
-                    (!SQR || ti <= tj);
+  const bool need = MODE == kColsLow ? ti + tj < C::Q : MODE == kColsHigh ? ti + tj >= C::Q - 2 : true;
   uint32_t v[8];
   if (need) {
     const uint4 xa = *reinterpret_cast<const uint4 *>(x + 4 * ti);
@@ -165,16 +166,16 @@ __device__ __forceinline__ void cta_cols(CtaSmem<N> &s, const uint32_t *x, const
   for (int j = tid; j < JOBS; j += C::THREADS) {
     const int d = D0 + (j >> 3), w = j & 7;
     const int lo = d > C::Q - 1 ? d - (C::Q - 1) : 0, hi = d < C::Q - 1 ? d : C::Q - 1;
+    // all Q loads of the diagonal in flight at once (predicated), two accumulators
     unsigned long long a0 = 0, a1 = 0;
 #pragma unroll
     for (int t = 0; t < C::Q; t++) {
-      const bool in = t >= lo && t <= hi && (!SQR || 2 * t <= d);
-      const unsigned long long v0 = s.tile[in ? (t * C::Q + (d - t)) * 9 + w : w];
-      const unsigned long long add = !in ? 0ull : (SQR && 2 * t < d) ? v0 << 1 : v0;
+      const bool in = t >= lo && t <= hi;
+      const uint32_t v0 = s.tile[in ? (t * C::Q + (d - t)) * 9 + w : w];
       if (t & 1)
-        a1 += add;
+        a1 += in ? v0 : 0u;
       else
-        a0 += add;
+        a0 += in ? v0 : 0u;
     }
     out[d * 8 + w] = a0 + a1;
   }
@@ -253,14 +254,11 @@ __device__ __forceinline__ void cta_resolve_n(CtaSmem<N> &s, Sum sum, uint32_t *
 // r = a b R^-1 mod N (a, b < N; or a, b < R with a b < R N).  r may alias a or b.
 template <int N>
 __device__ __forceinline__ void mont_cta(CtaSmem<N> &s, uint32_t *r, const uint32_t *a, const uint32_t *b) {
-  if (a == b)
-    cta_cols<N, kColsFull, true>(s, a, a, s.dsumT);
-  else
-    cta_cols<N, kColsFull, false>(s, a, b, s.dsumT);
+  cta_cols<N, kColsFull>(s, a, b, s.dsumT);
   cta_resolve_n<N, false>(s, [&](int i) { return cta_ws<N>(s.dsumT, i); }, s.t);  // T mod R
-  cta_cols<N, kColsLow, false>(s, s.t, s.np, s.dsum);
+  cta_cols<N, kColsLow>(s, s.t, s.np, s.dsum);
   cta_resolve_n<N, false>(s, [&](int i) { return cta_ws<N>(s.dsum, i); }, s.m);  // m
-  cta_cols<N, kColsHigh, false>(s, s.m, s.n, s.dsum);
+  cta_cols<N, kColsHigh>(s, s.m, s.n, s.dsum);
   // carry into word n from U's low half (which is 0 mod R)
   const unsigned long long sl = cta_ws<N>(s.dsum, N - 1) + cta_ws<N>(s.dsumT, N - 1);
   const unsigned long long carry = (sl >> 32) + ((sl & 0xffffffffull) != 0ull);
@@ -281,9 +279,9 @@ __device__ __forceinline__ void cta_neg_inverse(CtaSmem<N> &s) {
   __syncthreads();
 #pragma unroll 1
   for (int words = 1; words < N; words *= 2) {
-    cta_cols<N, kColsLow, false>(s, s.n, s.np, s.dsum);
+    cta_cols<N, kColsLow>(s, s.n, s.np, s.dsum);
     cta_resolve_n<N, false>(s, [&](int j) { return cta_ws<N>(s.dsum, j) + (j == 0 ? 2ull : 0ull); }, s.m);
-    cta_cols<N, kColsLow, false>(s, s.np, s.m, s.dsum);
+    cta_cols<N, kColsLow>(s, s.np, s.m, s.dsum);
     cta_resolve_n<N, false>(s, [&](int j) { return cta_ws<N>(s.dsum, j); }, s.np);
   }
 }
