@@ -821,14 +821,20 @@ def elementwise_suite(h, stream, steps, warmup, imad_peak):
 
     def timed(fn):
         """Median device time of one call.  Every step is queued behind an L2
-        flush (a 252 MB write), so the GPU never waits for the host inside the
-        events and no step finds its operands in L2; one synchronize at the end."""
+        flush (a 252 MB write), so no step finds its operands in L2, and behind
+        a 100 us device spin before its first event, so the GPU is still busy
+        while the host makes the library call: the events then bracket the
+        call's kernels alone, not the host's time to issue them (a few tens
+        of microseconds through ctypes, as long as the shortest kernels here).
+        One synchronize at the end."""
+        spin = int(100e-6 * torch.cuda.get_device_properties(0).clock_rate * 1e3)
         for _ in range(warmup):
             fn()
         torch.cuda.synchronize()
         evs = []
         for _ in range(steps):
             flush.zero_()
+            torch.cuda._sleep(spin)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             fn()
