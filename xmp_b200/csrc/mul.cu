@@ -47,15 +47,40 @@ __device__ __forceinline__ void store_limbs(const uint32_t (&x)[N], const OutVie
   for (uint32_t g = (N + 3) / 4; g < groups; g++) store_group(c.limbs, c.nlimbs, c.stride, e, g, make_uint4(0, 0, 0, 0));
 }
 
-template <int AL, int BL>
+// FAST: every operand holds exactly its class's limbs in whole 16-byte groups, no index arrays, no
+// broadcast -- instance i reads and writes element i with plain 128-bit accesses (no masking,
+// remainders or range checks: a quarter fewer instructions than the general form at 512 x 512).
+template <int AL, int BL, bool FAST>
 __global__ void __launch_bounds__(256) mul_reg_kernel(ArrayView a, ArrayView b, OutView c, uint32_t count) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
-  uint32_t ea = in_element(a, i), eb = in_element(b, i), ec = out_element(c, i);
-  if (ec >= c.count) return;
   uint32_t A[AL], B[BL], P[AL + BL];
-  load_limbs<AL>(A, a, ea);
-  load_limbs<BL>(B, b, eb);
+  uint32_t ec = i;
+  if constexpr (FAST) {
+    const uint4 *pa = reinterpret_cast<const uint4 *>(a.limbs) + i, *pb = reinterpret_cast<const uint4 *>(b.limbs) + i;
+#pragma unroll
+    for (int g = 0; g < AL / 4; g++) {
+      const uint4 q = pa[(size_t)g * a.stride];
+      A[4 * g] = q.x;
+      A[4 * g + 1] = q.y;
+      A[4 * g + 2] = q.z;
+      A[4 * g + 3] = q.w;
+    }
+#pragma unroll
+    for (int g = 0; g < BL / 4; g++) {
+      const uint4 q = pb[(size_t)g * b.stride];
+      B[4 * g] = q.x;
+      B[4 * g + 1] = q.y;
+      B[4 * g + 2] = q.z;
+      B[4 * g + 3] = q.w;
+    }
+  } else {
+    const uint32_t ea = in_element(a, i), eb = in_element(b, i);
+    ec = out_element(c, i);
+    if (ec >= c.count) return;
+    load_limbs<AL>(A, a, ea);
+    load_limbs<BL>(B, b, eb);
+  }
 #pragma unroll
   for (int k = 0; k < AL + BL; k++) P[k] = 0;
   // Row j adds A * B[j] at word j: the AL products are one mul.wide each (the
@@ -81,7 +106,14 @@ __global__ void __launch_bounds__(256) mul_reg_kernel(ArrayView a, ArrayView b, 
       P[j + AL] += (uint32_t)(p[0] >> 32);
     }
   }
-  store_limbs<AL + BL>(P, c, ec);
+  if constexpr (FAST) {
+    uint4 *pc = reinterpret_cast<uint4 *>(c.limbs) + i;
+#pragma unroll
+    for (int g = 0; g < (AL + BL) / 4; g++)
+      pc[(size_t)g * c.stride] = make_uint4(P[4 * g], P[4 * g + 1], P[4 * g + 2], P[4 * g + 3]);
+  } else {
+    store_limbs<AL + BL>(P, c, ec);
+  }
 }
 
 // Column k of the product, accumulated from the interleaved arrays.
@@ -117,7 +149,14 @@ __global__ void __launch_bounds__(256) mul_stream_kernel(ArrayView a, ArrayView 
 typedef void (*MulLaunch)(ArrayView, ArrayView, OutView, uint32_t, int, cudaStream_t);
 template <int AL, int BL>
 static void launch_mul(ArrayView a, ArrayView b, OutView c, uint32_t count, int threads, cudaStream_t s) {
-  mul_reg_kernel<AL, BL><<<grid_for(count, threads), threads, 0, s>>>(a, b, c, count);
+  if constexpr (AL % 4 == 0 && BL % 4 == 0) {
+    if (!a.index && !b.index && !c.index && a.nlimbs == (uint32_t)AL && b.nlimbs == (uint32_t)BL &&
+        c.nlimbs == (uint32_t)(AL + BL) && a.count >= count && b.count >= count && c.count >= count) {
+      mul_reg_kernel<AL, BL, true><<<grid_for(count, threads), threads, 0, s>>>(a, b, c, count);
+      return;
+    }
+  }
+  mul_reg_kernel<AL, BL, false><<<grid_for(count, threads), threads, 0, s>>>(a, b, c, count);
 }
 
 static const int kClasses[] = {2, 4, 8, 12, 16, 24, 32};
