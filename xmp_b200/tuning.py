@@ -254,14 +254,18 @@ def analytic_window(exp_bits, wmax=7, sliding=True):
 
 
 def runtime_slot(shape, slot):
-    """The configuration the library runs for a selector choice: for powm the chosen kernel with
-    the analytic window (capped at the six windows the tuner times).  Register kernels take the
+    """The configuration the library runs for a selector choice (tuner_lookup_powm): for powm the
+    chosen kernel with the chosen window kept within one of the analytic window's (the analytic
+    window alone where it is beyond the six windows the tuner times).  Register kernels take the
     sliding-window rule here; the fixed-window kernels' rule gives the same window at every
     exponent length of the dataset (17, 256, 1024 and the full precisions)."""
     if shape[0] != OPS["powm"]:
         return slot
-    d = slot // 6
-    return d * 6 + min(analytic_window(shape[2], sliding=d < 6), 6) - 1
+    d, w = slot // 6, slot % 6 + 1
+    wa = analytic_window(shape[2], sliding=d < 6)
+    if wa > 6:
+        return d * 6 + 5
+    return d * 6 + max(wa - 1, min(wa + 1, w)) - 1
 
 
 def regret_of(ms_row, slot):
