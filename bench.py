@@ -281,6 +281,33 @@ def config1_suite(h, stream, flush, steps, warmup, imad_peak, cpu_seconds):
             "result_check": ok}
 
 
+def sweep_suite(h, stream, flush, imad_peak, counts=(4096, 16384, 65536, 262144), steps=3):
+    """The 2048-bit workload (full-length exponents) over batch sizes 2^12 .. 2^18: modexp/s and the
+    IMAD roofline fraction per size with the library's default choice, 32 results per size checked
+    against GMP."""
+    import oracle as orc
+    import xmp_b200 as xmp
+    bits, n = 2048, 64
+    out = {}
+    for count in counts:
+        x, e, m = make_inputs(bits, count)
+        X, E, M, O = (h.integers(bits, count) for _ in range(4))
+        for arr, rows in ((X, x), (E, e), (M, m)):
+            arr.import_(rows)
+        cfg = xmp.powm_get_config(h, bits, bits, count)
+        step = lambda: xmp.check(xmp.lib().xmpIntegersPowmAsync(h.h, O.x, X.x, E.x, M.x, count), "xmpIntegersPowmAsync")
+        ms = statistics.median(_timed_events(step, stream, flush, steps, 1))
+        want, _ = orc.powm(x[:32], e[:32], m[:32], 32)
+        ok = bool(np.array_equal(O.export()[:32], want))
+        achieved = imad_per_modexp(bits, bits) * count / (ms * 1e-3) / 1e12
+        out[str(count)] = {"value": count / (ms * 1e-3), "unit": "modexp/s", "ms": ms, "imad_frac": achieved / imad_peak,
+                           "kernel": {"distribution": cfg.distribution, "lanes": cfg.lanes, "limbs": cfg.limbs,
+                                      "window": cfg.window}, "check": ok}
+        for v in (X, E, M, O):
+            v.destroy()
+    return out
+
+
 def latency_suite(h, stream, reps=5):
     """One full-exponent modexp alone, per size, through xmpIntegersPowm: the library's default
     choice for a batch of one (one instance per CTA) and the fastest lane kernel for it (the
@@ -491,6 +518,7 @@ def run_ours(args, rank, world, local_rank):
                                         "imad_peak_timad_s": peaks["imad"]}
         extra["config3_mixed"] = mixed_suite(3, 1, 65536, 16384, 256)
         extra["single_op_latency"] = latency_suite(h, stream)
+        extra["powm2048_batch_sweep"] = sweep_suite(h, stream, flush, peaks["imad"])
         extra["seconds"] = time.perf_counter() - t0
 
     line = {

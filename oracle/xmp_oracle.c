@@ -104,7 +104,7 @@ enum { OP_ADD = 0, OP_SUB, OP_AND, OP_IOR, OP_XOR, OP_MUL, OP_DIV, OP_MOD };
 /* out = op(a, b) mod 2^(32 out.n) for `count` instances. */
 int oracle_binary(int op, orc_out out, orc_in a, orc_in b, uint32_t count, int threads) {
   int bad = 0;
-  if (threads > 0) omp_set_num_threads(threads);
+  omp_set_num_threads(threads > 0 ? threads : omp_get_num_procs());
 #pragma omp parallel
   {
     mpz_t x, y, r, q;
@@ -156,7 +156,7 @@ int oracle_binary(int op, orc_out out, orc_in a, orc_in b, uint32_t count, int t
 
 /* q = floor(a / b), r = a mod b; division by zero gives q = a, r = 0. */
 int oracle_divmod(orc_out qo, orc_out ro, orc_in a, orc_in b, uint32_t count, int threads) {
-  if (threads > 0) omp_set_num_threads(threads);
+  omp_set_num_threads(threads > 0 ? threads : omp_get_num_procs());
 #pragma omp parallel
   {
     mpz_t x, y, q, r;
@@ -247,7 +247,8 @@ int oracle_popc(uint32_t *c, orc_in a, uint32_t count) {
  * OpenMP threads (<= 0: all).  Returns the number of threads used. */
 int oracle_powm(orc_out out, orc_in base, orc_in ex, orc_in mod, uint32_t count, int threads, int mode) {
   int used = 1;
-  if (threads > 0) omp_set_num_threads(threads);
+  /* the thread count is set on every call: an earlier call's count would otherwise persist */
+  omp_set_num_threads(threads > 0 ? threads : omp_get_num_procs());
 #pragma omp parallel
   {
 #pragma omp single
