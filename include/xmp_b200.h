@@ -22,9 +22,10 @@ extern "C" {
  *                 distribution), 1 = digit-serial (lanes/limbs ignored),
  *                 2 = one instance per CTA (moduli up to 4096 bits; the library
  *                 sets limbs to the CTA's operand size, 32/64/96/128, and
- *                 ignores lanes) -- the lowest latency for a small batch, and
- *                 the default choice for batches of up to one (1024-bit and
- *                 smaller moduli) or two (larger) instances per SM;
+ *                 ignores lanes) -- the lowest latency for a small batch of
+ *                 moduli above 512 bits, and the default choice there for
+ *                 batches of up to two (2048-bit and smaller moduli) or one
+ *                 (larger) instances per SM;
  *   window:       exponent window bits, 1..7. */
 typedef struct {
   int32_t distribution;

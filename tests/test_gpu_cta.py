@@ -82,6 +82,8 @@ def test_cta_default_choice(handle):
     assert xmp.powm_get_config(handle, 1536, 1536, 16).distribution == 2
     assert xmp.powm_get_config(handle, 2048, 2048, 65536).distribution == 0
     assert xmp.powm_get_config(handle, 8192, 8192, 1).distribution != 2  # beyond 4096 bits
+    assert xmp.powm_get_config(handle, 512, 512, 1).distribution != 2  # small moduli: the lane kernels
+    assert xmp.powm_get_config(handle, 544, 544, 1).distribution == 2
 
 
 def test_cta_through_the_default_call_with_indices_and_in_place(handle):

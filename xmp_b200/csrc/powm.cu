@@ -45,7 +45,11 @@ int window_for_bits(uint32_t exp_bits, bool sliding) {
 
 bool powm_cta_preferred(uint32_t nlimbs, uint32_t count, uint32_t sm_count) {
   const uint32_t limbs = powm_cta_limbs(nlimbs);
-  if (!limbs) return false;
+  // Up to 512 bits the smallest CTA (1024-bit operands) pads too much: one instance measured 0.34 /
+  // 0.69 / 1.12 ms at 64 / 256 / 512 bits against 0.017 / 0.18 / 0.61 ms on the lane kernels; from
+  // 544 bits on it is faster at every measured size (544: 1.17 vs 1.20 ms, 1056: 2.56 vs 2.97,
+  // 1536: 3.49 vs 4.20, 2080: 6.95 vs 11.0, 3104: 17.7 vs 23.4 ms).
+  if (!limbs || nlimbs <= 16) return false;
   // A CTA per instance runs it at its lone latency while the SMs hold the batch; the lane kernels
   // need thousands of instances before their throughput beats that.  Measured on B200 through
   // xmpIntegersPowm (full-length exponents), CTA vs the fastest lane kernel at 1 / 148 / 296 / 444

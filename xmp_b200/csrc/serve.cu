@@ -229,7 +229,8 @@ static void choose_configs(xmpServer_t s, Class &c) {
     // latency -- only up to 2048 bits, where that form beats the lane kernels alone (one op: 5.8 vs
     // 8.4 ms at 2048 bits; 3072 bits 15.1 vs 16.4, 4096 bits 31.6 vs 30.7 ms)
     c.cta_limbs = powm_cta_limbs(c.n);
-    c.cta[b] = c.cta_limbs != 0 && c.cta_limbs <= 64 && ops <= s->h->sm_count;
+    c.cta[b] = c.cta_limbs != 0 && c.cta_limbs <= 64 && ops <= s->h->sm_count &&
+               powm_cta_preferred(c.n, ops, s->h->sm_count);
   }
 }
 
