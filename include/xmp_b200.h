@@ -24,8 +24,8 @@ extern "C" {
  *                 sets limbs to the CTA's operand size, 32/64/96/128, and
  *                 ignores lanes) -- the lowest latency for a small batch of
  *                 moduli above 512 bits, and the default choice there for
- *                 batches of up to two (2048-bit and smaller moduli) or one
- *                 (larger) instances per SM;
+ *                 batches of up to 4-6 (1024-bit and smaller moduli), 2-3
+ *                 (up to 2048 bits) or one (larger) instances per SM;
  *   window:       exponent window bits, 1..7. */
 typedef struct {
   int32_t distribution;

@@ -2,15 +2,20 @@
 (xmp_b200/csrc/cta.cuh), step by step with Python integers:
 
 * each multiplication as 4 x 4-limb tiles summed per anti-diagonal word
-  (64-bit column sums, no carries), with the tile subsets the kernel forms
-  (all; the low half for m; the diagonals from n/4 - 2 up for m N);
+  (64-bit column sums, no carries) into the kernel's word-linear buffers (low
+  and high tile halves apart, four zero words either side, the buffers kept
+  from one product to the next as in shared memory, so a schedule that read a
+  word its product did not write would read a stale one), with the tile
+  subsets the kernel forms (all; the low half for m; the diagonals from
+  n/4 - 2 up for m N, T's sums added in by the same jobs);
 * the single-warp resolution: 32 lanes x n/32 words, the bits above 32 of the
   two words below folded in, the remaining one-bit carries by the ballot
   lookahead (P + 2G) xor P, and the value above the top word;
 * the schedule: T's low half resolved, m = T N' mod R, U = T + m N with T's
   high half entering as raw column sums and U's low half replaced by the carry
-  identity hi(s) + (lo(s) != 0) of word n - 1, then the conditional
-  subtraction of N with the lane-wise borrow lookahead;
+  identity hi(s) + (lo(s) != 0) of word n - 1 (entering as the high half of
+  that word's sum), then the conditional subtraction of N with the lane-wise
+  borrow lookahead;
 * N' by Newton's iteration y <- y (2 + N y) from -N^-1 mod 2^32.
 
 Every result is compared with a b R^-1 mod N; moduli of full length, with
@@ -34,27 +39,29 @@ class Cta:
     def __init__(self, n):
         self.n, self.q = n, n // 4
         self.diag = 2 * self.q - 1
+        # column sums, word i at [4 + i] of lo (tile words 0-3) and hi (tile words 4-7)
+        self.dsum = ([0] * (2 * n + 8), [0] * (2 * n + 8))
+        self.dsumT = ([0] * (2 * n + 8), [0] * (2 * n + 8))
 
-    def columns(self, x, y, mode):
+    def columns(self, x, y, mode, out, merge=None):
         q = self.q
         d0 = q - 2 if mode == "high" else 0
         d1 = q if mode == "low" else self.diag
-        ds = [None] * (self.diag * 8)
         for d in range(d0, d1):
             lo, hi = max(0, d - (q - 1)), min(d, q - 1)
             tiles = [words(val(x[4 * t:4 * t + 4]) * val(y[4 * (d - t):4 * (d - t) + 4]), 8) for t in range(lo, hi + 1)]
             for w in range(8):
-                ds[d * 8 + w] = sum(t[w] for t in tiles)
-        return ds
+                half = 0 if w < 4 else 1
+                v = sum(t[w] for t in tiles)
+                if merge is not None:
+                    v += merge[half][4 + 4 * d + w]
+                out[half][4 + 4 * d + w] = v
+        return out
 
-    def ws(self, buf, i):
-        if i < 0:
-            return 0
-        d, w = i >> 2, i & 3
-        a = buf[d * 8 + w] if d < self.diag else 0
-        if d >= 1:
-            a += buf[(d - 1) * 8 + w + 4]
-        return a
+    @staticmethod
+    def ws(buf, i):
+        assert -4 <= i < len(buf[0]) - 4
+        return buf[0][4 + i] + buf[1][4 + i]
 
 
 def resolve(nwords, sumf):
@@ -115,16 +122,18 @@ def sub_if(u, nw, top):
     return out
 
 
+def low_carry(v):
+    return ((v >> 32) + int((v & M32) != 0)) << 32
+
+
 def mont(c, a, b, nw, npw):
     n = c.n
-    dt = c.columns(a, b, "full")
+    dt = c.columns(a, b, "full", c.dsumT)
     t, _ = resolve(n, lambda i: c.ws(dt, i))
-    dm = c.columns(t, npw, "low")
+    dm = c.columns(t, npw, "low", c.dsum)
     m, _ = resolve(n, lambda i: c.ws(dm, i))
-    du = c.columns(m, nw, "high")
-    sl = c.ws(du, n - 1) + c.ws(dt, n - 1)
-    carry = (sl >> 32) + int((sl & M32) != 0)
-    u, top = resolve(n, lambda j: 0 if j < 0 else c.ws(du, n + j) + c.ws(dt, n + j) + (carry if j == 0 else 0))
+    du = c.columns(m, nw, "high", c.dsum, merge=dt)
+    u, top = resolve(n, lambda j: 0 if j < -1 else low_carry(c.ws(du, n - 1)) if j == -1 else c.ws(du, n + j))
     return sub_if(u, nw, top)
 
 
@@ -134,9 +143,9 @@ def neg_inverse(c, nw):
     y[0] = (-pow(nw[0], -1, 1 << 32)) & M32
     w = 1
     while w < n:
-        d = c.columns(nw, y, "low")
+        d = c.columns(nw, y, "low", c.dsum)
         m, _ = resolve(n, lambda j: c.ws(d, j) + (2 if j == 0 else 0))
-        d = c.columns(y, m, "low")
+        d = c.columns(y, m, "low", c.dsum)
         y, _ = resolve(n, lambda j: c.ws(d, j))
         w *= 2
     return y

@@ -10,11 +10,12 @@
 //   T = a b,   m = (T mod R) N' mod R   (N' = -N^-1 mod R),   U = T + m N,
 //   r = U / R  (< 2N; one conditional subtraction of N makes it < N).
 // Each product x y (n words each) is cut into 4 x 4-word tiles, one per thread
-// (16 mul.wide and two carry chains give the tile's exact 8-word product);
-// the tiles on one anti-diagonal share a word offset, so thread (d, w) sums
-// word w of the tiles of diagonal d (64-bit accumulators, no carries yet);
-// one warp then resolves n words, K = n/32 per lane: each word's two diagonal
-// sums, the bits above 32 of the two words below folded in, and the remaining
+// (16 mul.wide; four row chains added as a tree give the tile's exact 8-word
+// product); the tiles on one anti-diagonal share a word offset, so thread
+// (d, w) sums word w of the tiles of diagonal d (64-bit accumulators, no
+// carries yet) into a word-linear array (low and high tile halves apart);
+// one warp then resolves n words, K = n/32 per lane: each word's column sum,
+// the bits above 32 of the two words below folded in, and the remaining
 // one-bit carries by a ballot lookahead (the incoming carries of 32 lanes are
 // the bits of (P + 2G + cin) xor P).  Of U only the high half is resolved and
 // of T only the low half (the product schedule below).  A product costs 3
@@ -38,12 +39,20 @@ struct CtaShape {
   static constexpr int WARPS = THREADS / 32;
 };
 
+// Column sums of a product, word i = lo[4 + i] + hi[4 + i]: lo takes the low four words of the
+// tiles (anti-diagonal d, word w < 4 -> i = 4 d + w), hi their high four (w >= 4 -> i = 4 d + w);
+// four zero words below word 0 and above word 2n - 1 (never written).
+template <int N>
+struct ColSums {
+  unsigned long long lo[2 * N + 8], hi[2 * N + 8];
+};
+
 // Shared memory of one CTA (the window table follows it, `entries` x N words).
 template <int N>
 struct CtaSmem {
-  uint32_t tile[CtaShape<N>::THREADS * 9];  // 8 words per tile, one pad word against bank conflicts
-  unsigned long long dsum[CtaShape<N>::DIAG * 8];   // column sums of the current product, per anti-diagonal word
-  unsigned long long dsumT[CtaShape<N>::DIAG * 8];  // those of T = a b, kept for U = T + m N
+  uint32_t tile[CtaShape<N>::THREADS * 8];  // 8 words per tile
+  ColSums<N> dsum;   // column sums of the current product
+  ColSums<N> dsumT;  // those of T = a b, kept for U = T + m N
   uint32_t flag[2][32];                     // per warp: carry out with no carry in, all-propagate
   uint32_t t[2 * N];                        // T = a b
   uint32_t m[N], u[N];                      // m; the high half of U before its final subtraction
@@ -57,26 +66,44 @@ __host__ __device__ constexpr uint32_t cta_smem_bytes(uint32_t entries) {
   return (uint32_t)sizeof(CtaSmem<N>) + entries * N * 4;
 }
 
-// v (8 words) = x (4 words) * y (4 words).
+// v (8 words) = x (4 words) * y (4 words): four row products x y_j (5 words, one carry chain
+// each, independent), added pairwise (rows 0 + 1, rows 2 + 3), then the two halves: a dependent
+// carry path of 4 + 5 + 6 additions instead of one chain through all 16 products.
+__device__ __forceinline__ void cta_row(uint32_t (&r)[5], const uint32_t (&x)[4], uint32_t y) {
+  const uint64_t p0 = mul_wide(x[0], y), p1 = mul_wide(x[1], y), p2 = mul_wide(x[2], y), p3 = mul_wide(x[3], y);
+  r[0] = (uint32_t)p0;
+  r[1] = add_cc((uint32_t)(p0 >> 32), (uint32_t)p1);
+  r[2] = addc_cc((uint32_t)(p1 >> 32), (uint32_t)p2);
+  r[3] = addc_cc((uint32_t)(p2 >> 32), (uint32_t)p3);
+  r[4] = addc((uint32_t)(p3 >> 32), 0u);
+}
+
+// a (6 words) = r (5 words) + q (5 words) * 2^32.
+__device__ __forceinline__ void cta_add_shift(uint32_t (&a)[6], const uint32_t (&r)[5], const uint32_t (&q)[5]) {
+  a[0] = r[0];
+  a[1] = add_cc(r[1], q[0]);
+  a[2] = addc_cc(r[2], q[1]);
+  a[3] = addc_cc(r[3], q[2]);
+  a[4] = addc_cc(r[4], q[3]);
+  a[5] = addc(q[4], 0u);
+}
+
 __device__ __forceinline__ void cta_tile(uint32_t (&v)[8], const uint32_t (&x)[4], const uint32_t (&y)[4]) {
-#pragma unroll
-  for (int k = 0; k < 8; k++) v[k] = 0;
-#pragma unroll
-  for (int j = 0; j < 4; j++) {
-    uint64_t p[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) p[k] = mul_wide(x[k], y[j]);
-    // words above j + 3 are still zero here: the partial product of rows < j is below 2^(32 (j + 4))
-    v[j] = add_cc(v[j], (uint32_t)p[0]);
-    v[j + 1] = addc_cc(v[j + 1], (uint32_t)p[1]);
-    v[j + 2] = addc_cc(v[j + 2], (uint32_t)p[2]);
-    v[j + 3] = addc_cc(v[j + 3], (uint32_t)p[3]);
-    v[j + 4] = addc(0u, 0u);
-    v[j + 1] = add_cc(v[j + 1], (uint32_t)(p[0] >> 32));
-    v[j + 2] = addc_cc(v[j + 2], (uint32_t)(p[1] >> 32));
-    v[j + 3] = addc_cc(v[j + 3], (uint32_t)(p[2] >> 32));
-    v[j + 4] = addc(v[j + 4], (uint32_t)(p[3] >> 32));
-  }
+  uint32_t r0[5], r1[5], r2[5], r3[5], A[6], B[6];
+  cta_row(r0, x, y[0]);
+  cta_row(r1, x, y[1]);
+  cta_row(r2, x, y[2]);
+  cta_row(r3, x, y[3]);
+  cta_add_shift(A, r0, r1);
+  cta_add_shift(B, r2, r3);
+  v[0] = A[0];
+  v[1] = A[1];
+  v[2] = add_cc(A[2], B[0]);
+  v[3] = addc_cc(A[3], B[1]);
+  v[4] = addc_cc(A[4], B[2]);
+  v[5] = addc_cc(A[5], B[3]);
+  v[6] = addc_cc(B[4], 0u);
+  v[7] = addc(B[5], 0u);
 }
 
 // Carry lookahead over W words held one per thread (threads [0, W)): word
@@ -138,16 +165,20 @@ __device__ __forceinline__ uint32_t cta_sub_if(CtaSmem<N> &s, uint32_t *r, const
 // exactly hi(s_i) + (lo(s_i) != 0) (the word itself must come out 0), so the
 // carry into word n is c = hi(s_(n-1)) + (lo(s_(n-1)) != 0) and only the words
 // >= n - 1 of U are summed.  T's high half is therefore never resolved either:
-// its raw diagonal sums (dsumT) enter U's column sums directly; only T's low
-// half is resolved (it is m's operand).  (Squarings that form only the tiles
-// on and above the tile grid's diagonal, counting the others twice, measured
-// slower: one 2048-bit exponentiation 4.76 against 4.42 ms -- the tile phase
-// does not get shorter and the diagonal sums pay for the extra predicates.)
+// its raw column sums (dsumT) are added into U's by the same jobs that sum
+// m N's diagonals; only T's low half is resolved (it is m's operand).
+// (Squarings that form only the tiles on and above the tile grid's diagonal,
+// counting the others twice, measured slower with the per-diagonal layout: one
+// 2048-bit exponentiation 4.76 against 4.42 ms -- the tile phase does not get
+// shorter and the diagonal sums pay for the extra predicates.  Sums over a
+// warp-uniform range of tiles instead of all n/4 with predicates, 64-bit
+// uncarried tile columns, and two-word jobs where one-word jobs fit the CTA
+// all measured slower than the form here.)
 enum CtaCols : int { kColsFull = 0, kColsLow = 1, kColsHigh = 2 };
 
 template <int N, int MODE>
 __device__ __forceinline__ void cta_cols(CtaSmem<N> &s, const uint32_t *x, const uint32_t *y,
-                                         unsigned long long *out) {
+                                         ColSums<N> &out) {
   using C = CtaShape<N>;
   const int tid = threadIdx.x, ti = tid / C::Q, tj = tid % C::Q;
   const bool need = MODE == kColsLow ? ti + tj < C::Q : MODE == kColsHigh ? ti + tj >= C::Q - 2 : true;
@@ -157,52 +188,84 @@ __device__ __forceinline__ void cta_cols(CtaSmem<N> &s, const uint32_t *x, const
     const uint4 yb = *reinterpret_cast<const uint4 *>(y + 4 * tj);
     const uint32_t xw[4] = {xa.x, xa.y, xa.z, xa.w}, yw[4] = {yb.x, yb.y, yb.z, yb.w};
     cta_tile(v, xw, yw);
-#pragma unroll
-    for (int w = 0; w < 8; w++) s.tile[tid * 9 + w] = v[w];
+    uint4 *tp = reinterpret_cast<uint4 *>(&s.tile[tid * 8]);
+    tp[0] = make_uint4(v[0], v[1], v[2], v[3]);
+    tp[1] = make_uint4(v[4], v[5], v[6], v[7]);
   }
   __syncthreads();
   constexpr int D0 = MODE == kColsHigh ? C::Q - 2 : 0, D1 = MODE == kColsLow ? C::Q : C::DIAG;
-  constexpr int JOBS = (D1 - D0) * 8;
+  constexpr bool PAIR = (D1 - D0) * 8 > C::THREADS;  // two words per job when one-word jobs outnumber the threads
+  constexpr int WPJ = PAIR ? 2 : 1, JOBS = (D1 - D0) * 8 / WPJ;
   for (int j = tid; j < JOBS; j += C::THREADS) {
-    const int d = D0 + (j >> 3), w = j & 7;
+    const int d = D0 + j / (8 / WPJ), w = (j % (8 / WPJ)) * WPJ;
     const int lo = d > C::Q - 1 ? d - (C::Q - 1) : 0, hi = d < C::Q - 1 ? d : C::Q - 1;
-    // all Q loads of the diagonal in flight at once (predicated), two accumulators
+    // all Q loads of the diagonal in flight at once (predicated)
     unsigned long long a0 = 0, a1 = 0;
+    unsigned long long *o = &(w < 4 ? out.lo : out.hi)[4 + 4 * d + w];
+    const unsigned long long *tt = &(w < 4 ? s.dsumT.lo : s.dsumT.hi)[4 + 4 * d + w];
+    if constexpr (PAIR) {
 #pragma unroll
-    for (int t = 0; t < C::Q; t++) {
-      const bool in = t >= lo && t <= hi;
-      const uint32_t v0 = s.tile[in ? (t * C::Q + (d - t)) * 9 + w : w];
-      if (t & 1)
-        a1 += in ? v0 : 0u;
-      else
-        a0 += in ? v0 : 0u;
+      for (int t = 0; t < C::Q; t++) {
+        const bool in = t >= lo && t <= hi;
+        const uint2 v = *reinterpret_cast<const uint2 *>(&s.tile[in ? (t * C::Q + (d - t)) * 8 + w : w]);
+        a0 += in ? v.x : 0u;
+        a1 += in ? v.y : 0u;
+      }
+      if constexpr (MODE == kColsHigh) {  // U = T + m N
+        const ulonglong2 t2 = *reinterpret_cast<const ulonglong2 *>(tt);
+        a0 += t2.x;
+        a1 += t2.y;
+      }
+      *reinterpret_cast<ulonglong2 *>(o) = make_ulonglong2(a0, a1);
+    } else {
+#pragma unroll
+      for (int t = 0; t < C::Q; t++) {
+        const bool in = t >= lo && t <= hi;
+        const uint32_t v0 = s.tile[in ? (t * C::Q + (d - t)) * 8 + w : w];
+        if (t & 1)
+          a1 += in ? v0 : 0u;
+        else
+          a0 += in ? v0 : 0u;
+      }
+      unsigned long long v = a0 + a1;
+      if constexpr (MODE == kColsHigh) v += *tt;  // U = T + m N
+      *o = v;
     }
-    out[d * 8 + w] = a0 + a1;
   }
   __syncthreads();
 }
 
-// Column sum of product word i from per-diagonal sums (0 for i < 0).
+// Column sum of product word i (-4 <= i < 2n + 4; 0 outside [0, 2n)).
 template <int N>
-__device__ __forceinline__ unsigned long long cta_ws(const unsigned long long *buf, int i) {
-  if (i < 0) return 0ull;
-  const int d = i >> 2, w = i & 3;
-  unsigned long long a = d < CtaShape<N>::DIAG ? buf[d * 8 + w] : 0ull;
-  if (d >= 1) a += buf[(d - 1) * 8 + w + 4];
-  return a;
+__device__ __forceinline__ unsigned long long cta_ws(const ColSums<N> &c, int i) {
+  return c.lo[4 + i] + c.hi[4 + i];
+}
+
+// Column sums of words i, i + 1 (i even) with two 16-byte loads.
+template <int N>
+__device__ __forceinline__ void cta_ws2(const ColSums<N> &c, int i, unsigned long long &v0, unsigned long long &v1) {
+  const ulonglong2 a = *reinterpret_cast<const ulonglong2 *>(&c.lo[4 + i]);
+  const ulonglong2 b = *reinterpret_cast<const ulonglong2 *>(&c.hi[4 + i]);
+  v0 = a.x + b.x;
+  v1 = a.y + b.y;
 }
 
 // One warp resolves n words whose column sums sum(j) (j = 0 .. n-1; 0 below)
 // are given, lane l words [lK, lK + K), K = n / 32 (as cta_resolve_warp).
 // SUB: then r = value - N if the value above word n - 1 is set or value >= N.
-template <int N, bool SUB, class Sum>
-__device__ __forceinline__ void cta_resolve_n(CtaSmem<N> &s, Sum sum, uint32_t *out) {
+template <int N, bool SUB, class Sum, class Sum2>
+__device__ __forceinline__ void cta_resolve_n(CtaSmem<N> &s, Sum sum, Sum2 sum2, uint32_t *out) {
   constexpr int K = N / 32;
   if (threadIdx.x < 32) {
     const int l = threadIdx.x, i0 = l * K;
     unsigned long long sm[K + 2];
+    if constexpr (K % 2 == 0) {
 #pragma unroll
-    for (int k = 0; k < K + 2; k++) sm[k] = sum(i0 - 2 + k);
+      for (int k = 0; k < K + 2; k += 2) sum2(i0 - 2 + k, sm[k], sm[k + 1]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < K + 2; k++) sm[k] = sum(i0 - 2 + k);
+    }
     unsigned long long x[K + 1];
 #pragma unroll
     for (int k = 0; k <= K; k++) x[k] = (sm[k + 1] & 0xffffffffull) + (sm[k] >> 32);
@@ -255,17 +318,31 @@ __device__ __forceinline__ void cta_resolve_n(CtaSmem<N> &s, Sum sum, uint32_t *
 template <int N>
 __device__ __forceinline__ void mont_cta(CtaSmem<N> &s, uint32_t *r, const uint32_t *a, const uint32_t *b) {
   cta_cols<N, kColsFull>(s, a, b, s.dsumT);
-  cta_resolve_n<N, false>(s, [&](int i) { return cta_ws<N>(s.dsumT, i); }, s.t);  // T mod R
+  cta_resolve_n<N, false>(
+      s, [&](int i) { return cta_ws<N>(s.dsumT, i); },
+      [&](int i, unsigned long long &v0, unsigned long long &v1) { cta_ws2<N>(s.dsumT, i, v0, v1); }, s.t);  // T mod R
   cta_cols<N, kColsLow>(s, s.t, s.np, s.dsum);
-  cta_resolve_n<N, false>(s, [&](int i) { return cta_ws<N>(s.dsum, i); }, s.m);  // m
-  cta_cols<N, kColsHigh>(s, s.m, s.n, s.dsum);
-  // carry into word n from U's low half (which is 0 mod R)
-  const unsigned long long sl = cta_ws<N>(s.dsum, N - 1) + cta_ws<N>(s.dsumT, N - 1);
-  const unsigned long long carry = (sl >> 32) + ((sl & 0xffffffffull) != 0ull);
+  cta_resolve_n<N, false>(
+      s, [&](int i) { return cta_ws<N>(s.dsum, i); },
+      [&](int i, unsigned long long &v0, unsigned long long &v1) { cta_ws2<N>(s.dsum, i, v0, v1); }, s.m);  // m
+  cta_cols<N, kColsHigh>(s, s.m, s.n, s.dsum);  // column sums of U from word n - 1 up
+  // Word n - 1 enters as its carry into word n, hi(s) + (lo(s) != 0) (U's low half is 0 mod R),
+  // placed in the high half of a sum whose low half is 0; words below it are 0.
+  const auto low_carry = [](unsigned long long v) {
+    return ((v >> 32) + ((v & 0xffffffffull) != 0ull)) << 32;
+  };
   cta_resolve_n<N, true>(
       s,
       [&](int j) {
-        return j < 0 ? 0ull : cta_ws<N>(s.dsum, N + j) + cta_ws<N>(s.dsumT, N + j) + (j == 0 ? carry : 0ull);
+        const unsigned long long v = cta_ws<N>(s.dsum, N + j);
+        return j < -1 ? 0ull : j == -1 ? low_carry(v) : v;
+      },
+      [&](int j, unsigned long long &v0, unsigned long long &v1) {
+        cta_ws2<N>(s.dsum, N + j, v0, v1);
+        if (j < 0) {  // j = -2: words n - 2, n - 1
+          v0 = 0ull;
+          v1 = low_carry(v1);
+        }
       },
       r);
 }
@@ -280,9 +357,17 @@ __device__ __forceinline__ void cta_neg_inverse(CtaSmem<N> &s) {
 #pragma unroll 1
   for (int words = 1; words < N; words *= 2) {
     cta_cols<N, kColsLow>(s, s.n, s.np, s.dsum);
-    cta_resolve_n<N, false>(s, [&](int j) { return cta_ws<N>(s.dsum, j) + (j == 0 ? 2ull : 0ull); }, s.m);
+    cta_resolve_n<N, false>(
+        s, [&](int j) { return cta_ws<N>(s.dsum, j) + (j == 0 ? 2ull : 0ull); },
+        [&](int j, unsigned long long &v0, unsigned long long &v1) {
+          cta_ws2<N>(s.dsum, j, v0, v1);
+          v0 += j == 0 ? 2ull : 0ull;
+        },
+        s.m);
     cta_cols<N, kColsLow>(s, s.np, s.m, s.dsum);
-    cta_resolve_n<N, false>(s, [&](int j) { return cta_ws<N>(s.dsum, j); }, s.np);
+    cta_resolve_n<N, false>(
+        s, [&](int j) { return cta_ws<N>(s.dsum, j); },
+        [&](int j, unsigned long long &v0, unsigned long long &v1) { cta_ws2<N>(s.dsum, j, v0, v1); }, s.np);
   }
 }
 
@@ -363,6 +448,10 @@ __global__ void __launch_bounds__(CtaShape<N>::THREADS) powm_cta_kernel(PowmArgs
     s.n[i] = load_limb(a.mod.limbs, a.mod.nlimbs, a.mod.stride, em, (uint32_t)i);
     s.x[i] = load_limb(a.base.limbs, a.base.nlimbs, a.base.stride, eb, (uint32_t)i);
     s.k[i] = i == 0 ? 1u : 0u;
+  }
+  {
+    unsigned long long *z = &s.dsum.lo[0];  // dsum and dsumT: 4 arrays of 2n + 8 words, contiguous
+    for (int w = i; w < 4 * (2 * N + 8); w += CtaShape<N>::THREADS) z[w] = 0ull;
   }
   __syncthreads();
   // x may be >= N (any base below R): x mod N comes out of Mont(x, R^2) = x R mod N

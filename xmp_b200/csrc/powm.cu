@@ -45,18 +45,22 @@ int window_for_bits(uint32_t exp_bits, bool sliding) {
 
 bool powm_cta_preferred(uint32_t nlimbs, uint32_t count, uint32_t sm_count) {
   const uint32_t limbs = powm_cta_limbs(nlimbs);
-  // Up to 512 bits the smallest CTA (1024-bit operands) pads too much: one instance measured 0.34 /
-  // 0.69 / 1.12 ms at 64 / 256 / 512 bits against 0.017 / 0.18 / 0.61 ms on the lane kernels; from
-  // 544 bits on it is faster at every measured size (544: 1.17 vs 1.20 ms, 1056: 2.56 vs 2.97,
-  // 1536: 3.49 vs 4.20, 2080: 6.95 vs 11.0, 3104: 17.7 vs 23.4 ms).
+  // Up to 512 bits the smallest CTA (1024-bit operands) pads too much: one instance measured 0.27 /
+  // 0.46 / 0.69 ms at 64 / 256 / 512 bits against 0.017 / 0.18 / 0.61 ms on the lane kernels; from
+  // 544 bits on it is faster at every measured size (544: 0.72 vs 1.20 ms, 1056: 1.82 vs 2.97,
+  // 1536: 2.42 vs 4.20, 2080: 5.54 vs 11.0, 3104: 13.9 vs 23.4, 4096: 17.7 vs 30.5 ms).
   if (!limbs || nlimbs <= 16) return false;
-  // A CTA per instance runs it at its lone latency while the SMs hold the batch; the lane kernels
+  // A CTA per instance runs it near its lone latency while the SMs hold the batch; the lane kernels
   // need thousands of instances before their throughput beats that.  Measured on B200 through
-  // xmpIntegersPowm (full-length exponents), CTA vs the fastest lane kernel at 1 / 148 / 296 / 444
-  // instances: 1024 bits 1.90/1.91/1.93/2.20 vs 2.13 ms; 2048 bits 5.08/5.12/6.42/11.2 vs 8.10 ms;
-  // 3072 bits 10.97/11.05/22.0 vs 15.9 ms; 4096 bits 25.3/25.6/51.2 vs 30.5 ms.  Up to 2048 bits
-  // two instances per SM fit (1024: 64 threads, 2048: 256 threads per CTA), above that one.
-  return count <= (limbs <= 64 ? 2u : 1u) * sm_count;
+  // xmpIntegersPowm (full-length exponents), CTA vs the lane kernel at 148 / 296 / 444 / 592 / 888 /
+  // 1184 instances: 768 bits -/-/-/1.12/1.36 vs 1.64/1.16 ms; 1024 bits 1.15/1.17/1.36/1.39/1.71/2.10
+  // vs 2.13 ms; 1280 bits 2.90 (296), 4.81 (370) vs 3.57 ms; 1536 bits 2.43/3.37/5.60 vs 4.21 ms;
+  // 1792 bits 3.84/6.37 (444) vs 7.15 ms; 2048 bits 3.08/4.30/7.15/8.57 vs 8.12 ms; 3072 bits
+  // 7.84/15.7 vs 16.0 ms; 4096 bits 17.8/35.6 vs 30.6 ms.
+  uint32_t per_sm = 1;
+  if (limbs == 32) per_sm = nlimbs > 24 ? 6 : 4;
+  else if (limbs == 64) per_sm = nlimbs > 48 ? 3 : 2;
+  return count <= per_sm * sm_count;
 }
 
 bool powm_config_valid(const PowmConfig &c, uint32_t nlimbs) {
