@@ -63,6 +63,7 @@ struct CtaSmem {
 
 template <int N>
 __host__ __device__ constexpr uint32_t cta_smem_bytes(uint32_t entries) {
+  static_assert(sizeof(CtaSmem<N>) % 16 == 0, "the window table after CtaSmem is read in 16-byte words");
   return (uint32_t)sizeof(CtaSmem<N>) + entries * N * 4;
 }
 
