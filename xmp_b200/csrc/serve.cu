@@ -226,11 +226,9 @@ static void choose_configs(xmpServer_t s, Class &c) {
     c.cfg[b] = cfg;
     c.entry[b] = powm_find(cfg.tpi, cfg.limbs);
     // small waves on a quiet GPU: one op per CTA (its constant-schedule form), at a lone op's lowest
-    // latency -- only up to 2048 bits, where that form beats the lane kernels alone (one op: 5.8 vs
-    // 8.4 ms at 2048 bits; 3072 bits 15.1 vs 16.4, 4096 bits 31.6 vs 30.7 ms)
+    // latency (one op: 3.6 vs 8.4 ms at 2048 bits, 9.2 vs 15.7 ms at 3072, 20.4 vs 30.0 ms at 4096)
     c.cta_limbs = powm_cta_limbs(c.n);
-    c.cta[b] = c.cta_limbs != 0 && c.cta_limbs <= 64 && ops <= s->h->sm_count &&
-               powm_cta_preferred(c.n, ops, s->h->sm_count);
+    c.cta[b] = c.cta_limbs != 0 && ops <= s->h->sm_count && powm_cta_preferred(c.n, ops, s->h->sm_count);
   }
 }
 
