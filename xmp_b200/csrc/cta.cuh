@@ -350,6 +350,14 @@ __device__ __forceinline__ void mont_cta(CtaSmem<N> &s, uint32_t *r, const uint3
       r);
 }
 
+// The same as a call: at 4096 bits the constant-schedule kernel's main loop, inlined, overflows
+// the instruction cache (one exponentiation 19.9 ms inlined, 18.5 ms as a call; everywhere else
+// the call measured slower: 2048 bits 3.46 -> 4.00 ms constant-schedule, 3.06 -> 3.95 sliding).
+template <int N>
+__device__ __noinline__ void mont_cta_call(CtaSmem<N> &s, uint32_t *r, const uint32_t *a, const uint32_t *b) {
+  mont_cta<N>(s, r, a, b);
+}
+
 // s.np = -N^-1 mod R by Newton's iteration y <- y (2 + N y), which doubles the
 // correct low words of y = -N^-1 each time (from -N^-1 mod 2^32).
 template <int N>
@@ -509,8 +517,12 @@ __global__ void __launch_bounds__(CtaShape<N>::THREADS) powm_cta_kernel(PowmArgs
     for (int32_t wi = (int32_t)nwin - 2; wi >= 0; wi--) {
       const uint32_t win = exp_window(a.exp, ee, (uint32_t)wi * W, W);
 #pragma unroll 1
-      for (uint32_t q = 0; q < W; q++) mont_cta<N>(s, s.acc, s.acc, s.acc);
-      mont_cta<N>(s, s.acc, s.acc, table + win * N);
+      for (uint32_t q = 0; q < W; q++) {
+        if constexpr (N == 128) mont_cta_call<N>(s, s.acc, s.acc, s.acc);
+        else mont_cta<N>(s, s.acc, s.acc, s.acc);
+      }
+      if constexpr (N == 128) mont_cta_call<N>(s, s.acc, s.acc, table + win * N);
+      else mont_cta<N>(s, s.acc, s.acc, table + win * N);
     }
   }
   mont_cta<N>(s, s.acc, s.acc, one);
