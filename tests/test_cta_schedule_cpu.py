@@ -171,3 +171,44 @@ def test_cta_montgomery_product(n):
             assert val(mont(c, words(a, n), words(a, n), nw, npw)) == a * a * rinv % mod
         x = rnd.randrange(r)  # any operand below R times R^2 mod N: x R mod N, fully reduced
         assert val(mont(c, words(x, n), words(r * r % mod, n), nw, npw)) == x * r % mod
+
+
+def tile_tree(x, y):
+    """The kernel's tile product (cta_tile): four row products x * y_j as 5-word chains, rows added
+    pairwise with one word of shift, then the halves with two; every add a 32-bit add with carry."""
+    def row(yj):
+        p = [xk * yj for xk in x]
+        r, c = [p[0] & M32], 0
+        for k in range(1, 4):
+            t = (p[k - 1] >> 32) + (p[k] & M32) + c
+            r.append(t & M32)
+            c = t >> 32
+        r.append(((p[3] >> 32) + c) & M32)
+        assert (p[3] >> 32) + c <= M32
+        return r
+
+    def add_shift(r, q, shift):
+        a, c = r[:shift], 0
+        for k in range(shift, len(r)):
+            t = r[k] + q[k - shift] + c
+            a.append(t & M32)
+            c = t >> 32
+        for k in range(len(r) - shift, len(q)):
+            t = q[k] + c
+            a.append(t & M32)
+            c = t >> 32
+        assert c == 0
+        return a
+
+    r0, r1, r2, r3 = (row(y[j]) for j in range(4))
+    A, B = add_shift(r0, r1, 1), add_shift(r2, r3, 1)
+    return add_shift(A, B, 2)
+
+
+def test_tile_tree_is_the_product():
+    rnd = random.Random(7)
+    cases = [([M32] * 4, [M32] * 4), ([0] * 4, [M32] * 4), ([1, 0, 0, 0], [M32] * 4)]
+    cases += [([rnd.getrandbits(32) for _ in range(4)], [rnd.getrandbits(32) for _ in range(4)]) for _ in range(2000)]
+    for x, y in cases:
+        v = tile_tree(x, y)
+        assert len(v) == 8 and val(v) == val(x) * val(y)

@@ -86,6 +86,16 @@ def test_cta_default_choice(handle):
     assert xmp.powm_get_config(handle, 544, 544, 1).distribution == 2
 
 
+def test_cta_default_batch_limits(handle):
+    """The batch sizes up to which one instance per CTA is the default (instances per SM, by the
+    CTA operand size and the modulus precision) and the first size past each limit."""
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    for bits, per_sm in ((768, 4), (1024, 6), (1536, 2), (2048, 3), (3072, 1), (4096, 1)):
+        assert xmp.powm_get_config(handle, bits, bits, per_sm * sms).distribution == 2, bits
+        assert xmp.powm_get_config(handle, bits, bits, per_sm * sms + 1).distribution != 2, bits
+
+
 def test_cta_through_the_default_call_with_indices_and_in_place(handle):
     bits, count = 2048, 24
     x, e, m = _case(990, count, bits)
