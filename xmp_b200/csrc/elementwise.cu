@@ -135,17 +135,22 @@ __global__ void __launch_bounds__(256) shf_smem_kernel(ArrayView a, OutView c, c
   }
   int64_t t = -(int64_t)shift[i % shift_count];
   int64_t q = (t >= 0) ? t / 32 : -((-t + 31) / 32);  // floor(t / 32)
-  uint32_t r = (uint32_t)(t - q * 32);
-  const int64_t na = a.nlimbs;
-  auto limb_at = [&](int64_t j) -> uint32_t { return (j < 0 || j >= na) ? 0u : col[j * 256 + tid]; };
+  const uint32_t r = (uint32_t)(t - q * 32);
   const uint32_t groups = div_up(c.nlimbs, 4);
-  uint32_t low = limb_at(q);
+  // Output limb k reads source limbs q + k and q + k + 1; a window that misses the operand entirely
+  // gives zeros.  Otherwise q fits 32 bits and one unsigned compare tests a limb index.
+  const int64_t reach = (int64_t)groups * 4 + 1;
+  if (q >= (int64_t)a.nlimbs || q + reach <= 0) q = -reach;
+  const int32_t q32 = (int32_t)q;
+  const uint32_t na = a.nlimbs;
+  auto limb_at = [&](int32_t j) -> uint32_t { return (uint32_t)j < na ? col[j * 256 + tid] : 0u; };
+  uint32_t low = limb_at(q32);
   for (uint32_t g = 0; g < groups; g++) {
     uint32_t out[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      uint32_t high = limb_at(q + (int64_t)(g * 4 + k) + 1);
-      out[k] = r ? __funnelshift_r(low, high, r) : low;
+      const uint32_t high = limb_at(q32 + (int32_t)(g * 4 + k) + 1);
+      out[k] = __funnelshift_r(low, high, r);  // r = 0 gives low
       low = high;
     }
     store_group(c.limbs, c.nlimbs, c.stride, ec, g, make_uint4(out[0], out[1], out[2], out[3]));
