@@ -29,6 +29,14 @@ enum class Bin { Add, Sub, And, Ior, Xor };
 // Grid-stride loops over instances: the launch covers at most the GPU's
 // resident threads (stream_grid), so each thread handles several instances
 // instead of the GPU launching and retiring one short-lived CTA per 256.
+// Input element of op instance i, as in_element, with each remainder taken only when it changes
+// the index: these kernels are light enough that two integer divisions per operand show (2-3 us
+// on shf and cmp over 2^22 instances).  The powm kernels keep in_element's plain remainders.
+__device__ __forceinline__ uint32_t ew_element(const ArrayView &v, uint32_t i) {
+  const uint32_t k = v.index ? v.index[i < v.index_count ? i : i % v.index_count] : i;
+  return k < v.count ? k : k % v.count;
+}
+
 #define XMPB_FOR_INSTANCES(i, count)                                                              \
   for (uint64_t i##_ = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i##_ < (count);            \
        i##_ += (uint64_t)gridDim.x * blockDim.x)
@@ -37,7 +45,7 @@ template <Bin OP>
 __global__ void __launch_bounds__(256) binary_kernel(ArrayView a, ArrayView b, OutView c, uint32_t count) {
   XMPB_FOR_INSTANCES(i, count) {
     const uint32_t i = (uint32_t)i_;
-    uint32_t ea = in_element(a, i), eb = in_element(b, i), ec = out_element(c, i);
+    uint32_t ea = ew_element(a, i), eb = ew_element(b, i), ec = out_element(c, i);
     if (ec >= c.count) continue;
     uint32_t groups = div_up(c.nlimbs, 4);
     uint32_t carry = (OP == Bin::Sub) ? 1u : 0u;  // subtraction as a + ~b + 1
@@ -72,7 +80,7 @@ __global__ void __launch_bounds__(256) binary_kernel(ArrayView a, ArrayView b, O
 __global__ void __launch_bounds__(256) not_kernel(ArrayView a, OutView c, uint32_t count) {
   XMPB_FOR_INSTANCES(i, count) {
     const uint32_t i = (uint32_t)i_;
-    uint32_t ea = in_element(a, i), ec = out_element(c, i);
+    uint32_t ea = ew_element(a, i), ec = out_element(c, i);
     if (ec >= c.count) continue;
     uint32_t groups = div_up(c.nlimbs, 4);
     for (uint32_t g = 0; g < groups; g++) {
@@ -87,7 +95,7 @@ __global__ void __launch_bounds__(256) shf_kernel(ArrayView a, OutView c, const 
                                                   uint32_t count) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
-  uint32_t ea = in_element(a, i), ec = out_element(c, i);
+  uint32_t ea = ew_element(a, i), ec = out_element(c, i);
   if (ec >= c.count) return;
   int64_t t = -(int64_t)shift[i % shift_count];
   int64_t q = (t >= 0) ? t / 32 : -((-t + 31) / 32);  // floor(t / 32)
@@ -123,7 +131,7 @@ __global__ void __launch_bounds__(256) shf_smem_kernel(ArrayView a, OutView c, c
   const uint32_t tid = threadIdx.x;
   uint32_t i = blockIdx.x * blockDim.x + tid;
   if (i >= count) return;
-  uint32_t ea = in_element(a, i), ec = out_element(c, i);
+  uint32_t ea = ew_element(a, i), ec = out_element(c, i);
   if (ec >= c.count) return;
   const uint32_t ag = div_up(a.nlimbs, 4);
   for (uint32_t g = 0; g < ag; g++) {
@@ -163,7 +171,7 @@ __global__ void __launch_bounds__(256) shf_smem_kernel(ArrayView a, OutView c, c
 __global__ void __launch_bounds__(256) cmp_kernel(ArrayView a, ArrayView b, int32_t *out, uint32_t count) {
   XMPB_FOR_INSTANCES(i, count) {
     const uint32_t i = (uint32_t)i_;
-    uint32_t ea = in_element(a, i), eb = in_element(b, i);
+    uint32_t ea = ew_element(a, i), eb = ew_element(b, i);
     uint32_t groups = div_up(max(a.nlimbs, b.nlimbs), 4);
     int32_t result = 0;
     for (int32_t g = (int32_t)groups - 1; g >= 0 && result == 0; g--) {
@@ -181,7 +189,7 @@ __global__ void __launch_bounds__(256) cmp_kernel(ArrayView a, ArrayView b, int3
 __global__ void __launch_bounds__(256) popc_kernel(ArrayView a, uint32_t *out, uint32_t count) {
   XMPB_FOR_INSTANCES(i, count) {
     const uint32_t i = (uint32_t)i_;
-    uint32_t ea = in_element(a, i);
+    uint32_t ea = ew_element(a, i);
     uint32_t groups = div_up(a.nlimbs, 4), s = 0;
     uint32_t g = 0;
     for (; g + 2 <= groups; g += 2) {  // two independent group loads in flight per thread

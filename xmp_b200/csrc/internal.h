@@ -47,7 +47,8 @@ struct OutView {
 // Input element selected by op instance i (docs 15-16; implementations.h:63-68).  (Taking the
 // remainders only when they change the index saved 2-3 us on shf and cmp over 2^22 instances but
 // moved the headline powm kernel's schedule: 240.1 against 237.8 ms per 65,536 x 2048-bit batch on
-// the same GPU; the multiply's whole-group path, where they mattered, skips this function.)
+// the same GPU; the elementwise kernels use their own such form, ew_element, and the multiply's
+// whole-group path skips this function.)
 __device__ __forceinline__ uint32_t in_element(const ArrayView &v, uint32_t i) {
   uint32_t k = v.index ? v.index[i % v.index_count] : i;
   return k % v.count;
