@@ -311,7 +311,7 @@ def sweep_suite(h, stream, flush, imad_peak, counts=(4096, 16384, 65536, 262144)
     return out
 
 
-def latency_suite(h, stream, reps=5):
+def latency_suite(h, stream, reps=5, sizes=(1024, 2048, 3072, 4096)):
     """One full-exponent modexp alone, per size, through xmpIntegersPowm: the library's default
     choice for a batch of one (one instance per CTA) and the fastest lane kernel for it (the
     warp-distributed heuristic), best of `reps` by CUDA events, both results checked against GMP."""
@@ -319,7 +319,7 @@ def latency_suite(h, stream, reps=5):
     import oracle as orc
     import xmp_b200 as xmp
     out = {}
-    for bits in (1024, 2048, 3072, 4096):
+    for bits in sizes:
         x, e, m = make_inputs(bits, 1)
         X, E, M, O = (h.integers(bits, 1) for _ in range(4))
         for arr, rows in ((X, x), (E, e), (M, m)):
@@ -1019,6 +1019,20 @@ def run_elementwise(args):
     h.destroy()
 
 
+def run_latency(args):
+    """One exponentiation alone per size (the latency suite of the default run, on its own)."""
+    import torch
+    import xmp_b200 as xmp
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    h = xmp.Handle()
+    h.set_stream(stream.cuda_stream)
+    sizes = tuple(int(b) for b in args.latency_bits.split(","))
+    print(json.dumps({"metric": "one full-exponent modexp alone", "unit": "ms",
+                      "sizes": latency_suite(h, stream, sizes=sizes)}), flush=True)
+    h.destroy()
+
+
 def run_crt(args):
     """CRT-RSA private operations (RSA-2048: 1024-bit primes from GMP nextprime on seeded starts,
     e = 65537, messages uniform below n): --count decryptions under --crt-keys keys through the
@@ -1072,7 +1086,9 @@ def main():
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="headline workload only (no config 1/2/3 or reference GPU)")
     ap.add_argument("--force-config", default=None, help="lanes,limbs,window: time this powm kernel configuration")
-    ap.add_argument("--workload", default="powm2048", choices=["powm2048", "mixed", "serve", "elementwise", "crt"])
+    ap.add_argument("--workload", default="powm2048",
+                    choices=["powm2048", "mixed", "serve", "elementwise", "crt", "latency"])
+    ap.add_argument("--latency-bits", default="1024,2048,3072,4096", help="latency workload: modulus sizes")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--serve-peak-requests", type=int, default=3000)
     ap.add_argument("--serve-sync-requests", type=int, default=40)
@@ -1092,6 +1108,9 @@ def main():
         return
     if args.workload == "crt":
         run_crt(args)
+        return
+    if args.workload == "latency":
+        run_latency(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
